@@ -1,0 +1,393 @@
+#!/usr/bin/env python
+"""Benchmark: propagated photons/s of the batched persistent kernel on the
+4096-pair mixed batch, next to the plain one-pair-per-launch path, the
+end-to-end C-ABI call with host buffers and the CPU baseline.
+
+One step = one propagation of a 4096-pair batch (photon counts log-uniform
+in [1e4, 1e7], 50/50 isotropic point / 1 m Cherenkov-cone emitters with
+random directions, sphere r = 0.21 m at a uniform distance in [2, 150] m in a
+random direction; seawater 35 permille / 2 degC, Frank-Tamm spectrum
+300-800 nm, HG g = 0.95, group-velocity time, PMT weighting, FP64 per-pair
+statistics and 1000 x 1 ns histograms).  Every step uses a fresh batch
+(different seeds).  Under torchrun each rank propagates its own batch (weak
+scaling, no collective on the data path).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+"""
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG_ROOT = os.path.join(REPO, "photonprop.jl_b200")
+for _p in (REPO, PKG_ROOT):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "propagated photons/s (batched vs plain, 1 B200); p50/p99 solve latency"
+UNIT = "photons/s"
+WORKLOAD = ("4096-pair mixed batch: photons/pair log-uniform [1e4,1e7], 50/50 isotropic point / 1 m "
+            "Cherenkov-cone emitters (random directions), sphere r=0.21 m at U[2,150] m in a random "
+            "direction; seawater 35 permille 2 degC, Frank-Tamm 300-800 nm, HG g=0.95, physical mode, "
+            "PMT weight, FP64 per-pair stats + 1000 x 1 ns histograms")
+RUN_KW = dict(mode="physical", g=0.95, t_max=1000.0, hist_t0=0.0, hist_bin_width=1.0, hist_bins=1000,
+              pmt_weight=True)
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--pairs", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-tune", action="store_true")
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled every 200 ms."""
+
+    FIELDS = ["uuid", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, uuid=None):
+        self.uuid = uuid
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) == len(self.FIELDS):
+                self.rows.append(parts)
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = self.rows
+        if self.uuid:
+            mine = [r for r in rows if self.uuid in r[0]]
+            rows = mine or rows
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+
+        def num(x):
+            try:
+                return float(x)
+            except ValueError:
+                return None
+        sm = [num(r[1]) for r in rows if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
+        pw = [num(r[3]) for r in rows if num(r[3]) is not None]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "power_w_max": max(pw) if pw else None, "samples": len(rows), "reasons": reasons}
+
+
+# ---------------------------------------------------------------------------
+def cpu_baseline(batch, target_seconds, run_kw):
+    """The FP64 CPU restatement of the reference kernel (oracle/, all host
+    threads) on a bounded sample of the same batch: the first L photons of
+    every pair, L chosen for about target_seconds of work."""
+    from oracle import oracle as O
+    from oracle import tables as tb
+    import photonprop_b200 as pp
+    m = tb.cascadia(35.0, 2.0)
+    knots = tb.cherenkov_spectrum_knots((300.0, 800.0), 20, m)
+    T = O.make_tables(m, knots, pmt=(pp.p_one_pmt_acc.wavelengths, pp.p_one_pmt_acc.acceptance))
+    op = O.pairs_array(len(batch))
+    for f in ("pos", "t0", "dir", "track_len", "target", "radius", "n_photons", "seed", "emitter"):
+        op[f] = batch[f]
+    oo = O.make_opts(mode=O.MODE_PHYSICAL, g=run_kw["g"], t_max=run_kw["t_max"], hist_bins=run_kw["hist_bins"],
+                     flags=O.OPT_PMT_WEIGHT)
+    cores = os.cpu_count() or 1
+    n = np.asarray(batch["n_photons"], dtype=np.int64)
+    lim = 64
+    t0 = time.perf_counter()
+    O.propagate(T, op, oo, photon_limit=lim, n_threads=cores)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    lim = int(max(64, min(n.max(), lim * target_seconds / dt)))
+    t0 = time.perf_counter()
+    O.propagate(T, op, oo, photon_limit=lim, n_threads=cores)
+    dt = time.perf_counter() - t0
+    photons = int(np.minimum(n, lim).sum())
+    return {"value": photons / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {lim} photons of each of the {len(batch)} pairs ({photons:.3e} photons, "
+                      f"{dt:.1f} s), FP64 oracle, OpenMP {cores} threads"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import photonprop_b200 as pp
+    steps, warm = args.steps, args.warmup
+    batch = pp.batches.mixed_batch(args.pairs, seed=args.seed)
+    per_step = max(2.0, min(args.cpu_seconds, 60.0 / max(steps + warm, 1)))
+    vals = []
+    base = None
+    for i in range(warm + steps):
+        b = cpu_baseline(batch, per_step, RUN_KW)
+        if i >= warm:
+            vals.append(b["value"])
+            base = b
+    v = statistics.median(vals)
+    base["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": steps, "warmup": warm, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "pairs": args.pairs, "sampled": True},
+            "cpu_baseline": base, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0},
+            "note": "the reference's propagation exists only as a CUDA.jl kernel (Julia is not installed); "
+                    "this arm times its FP64 C restatement on the host cores"}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import photonprop_b200 as pp
+    from photonprop_b200 import roofline
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def reduce(x, op):
+        if world == 1:
+            return x
+        t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=op)
+        return float(t.item())
+
+    SUM = dist.ReduceOp.SUM if world > 1 else None
+    MAX = dist.ReduceOp.MAX if world > 1 else None
+
+    peaks = pp.measure_peaks(local)
+    medium = pp.make_seawater(35.0, 2.0)
+    spec = pp.CherenkovSpectrum((300.0, 800.0), 20, medium)
+    prop = pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=local)
+    ro = pp.RunOptions(**RUN_KW)
+    W, K = args.warmup, args.steps
+    batches = [pp.batches.mixed_batch(args.pairs, seed=args.seed + 7919 * rank + i) for i in range(W + K)]
+    n_pairs = args.pairs
+    bins = RUN_KW["hist_bins"]
+
+    tune = None
+    if not args.no_tune:
+        sample = batches[0][:512].copy()
+        sample["n_photons"] = np.minimum(sample["n_photons"], 2_000_000)
+        tune = prop.autotune(sample, ro)
+        ro.block_size, ro.blocks_per_sm, ro.chunk_photons = (tune["block_size"], tune["blocks_per_sm"],
+                                                             tune["chunk_photons"])
+
+    cap = 1 << 22
+    d_pairs = [torch.from_numpy(b.view(np.uint8).copy()).to(dev) for b in batches]
+    d_hits = torch.empty(cap * 64, dtype=torch.uint8, device=dev)
+    d_cnt = torch.zeros(4, dtype=torch.int64, device=dev)
+    d_stats = torch.zeros((n_pairs, 8), dtype=torch.float64, device=dev)
+    d_hist = torch.zeros((n_pairs, bins), dtype=torch.float64, device=dev)
+    cnt_log = torch.zeros((K, 4), dtype=torch.int64, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)  # > 126 MB L2
+    s = torch.cuda.Stream(device=dev)
+
+    for i in range(W):
+        prop.propagate_device(d_pairs[i], n_pairs, ro, d_hits, cap, d_cnt, d_stats, d_hist, stream=s)
+    s.synchronize()
+    barrier()
+
+    uuid = None
+    try:
+        uuid = str(torch.cuda.get_device_properties(local).uuid)
+    except Exception:
+        pass
+    sampler = ClockSampler(uuid)
+    sampler.start()
+    time.sleep(0.3)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    launches0 = pp.launch_count()
+    torch.cuda.synchronize()
+    barrier()
+    t_wall = time.perf_counter()
+    for k in range(K):
+        with torch.cuda.stream(s):
+            flush.fill_(k & 0xFF)
+        ev[k][0].record(s)
+        prop.propagate_device(d_pairs[W + k], n_pairs, ro, d_hits, cap, d_cnt, d_stats, d_hist, stream=s)
+        ev[k][1].record(s)
+        with torch.cuda.stream(s):
+            cnt_log[k].copy_(d_cnt)
+    s.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    wall = time.perf_counter() - t_wall
+    launches = pp.launch_count() - launches0
+    clocks = sampler.stop()
+
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    cnt = cnt_log.cpu().numpy()
+    photons_local = [int(batches[W + k]["n_photons"].sum()) for k in range(K)]
+    t_local = sum(step_ms) / 1e3
+    t_max = reduce(t_local, MAX)
+    photons_all = reduce(sum(photons_local), SUM)
+    value = photons_all / t_max
+    # roofline of the batched launch sequence (the batched kernel is >99.9 % of it)
+    iso = [int(batches[W + k]["n_photons"][batches[W + k]["emitter"] == 0].sum()) for k in range(K)]
+    cone = [photons_local[k] - iso[k] for k in range(K)]
+    steps_total = int(cnt[:, 1].sum())
+    mufu, fp32, iops = roofline.op_counts(steps_total, sum(iso), sum(cone))
+    a_mufu, a_fp32, a_int = mufu / t_local, fp32 / t_local, iops / t_local
+    f_mufu, f_fp32 = a_mufu / peaks["mufu_ops"], a_fp32 / peaks["fp32_ops"]
+    hits_local = int(cnt[:, 0].sum())
+
+    # plain: one launch per pair on the same batch, kernels only (no host sync
+    # between pairs) and through the host-buffer API (sync + copy-back per pair)
+    plain = None
+    if not args.no_plain:
+        b = batches[W]
+        h_pairs = [b[i:i + 1].copy() for i in range(n_pairs)]
+        d_pair_views = [d_pairs[W][i * 80:(i + 1) * 80] for i in range(n_pairs)]
+        d_st1 = torch.zeros((1, 8), dtype=torch.float64, device=dev)
+        d_hi1 = torch.zeros((1, bins), dtype=torch.float64, device=dev)
+
+        def plain_pass():
+            for i in range(n_pairs):
+                prop.propagate_plain_device(d_pair_views[i], h_pairs[i], i, ro, d_hits, cap, d_cnt, d_st1, d_hi1,
+                                            stream=s)
+        plain_pass()  # warm-up
+        s.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(s):
+            flush.fill_(1)
+        e0.record(s)
+        plain_pass()
+        e1.record(s)
+        s.synchronize()
+        t_pk = e0.elapsed_time(e1) / 1e3
+        hits_np = np.zeros(cap, dtype=pp.HIT_DTYPE)
+        st_np = np.zeros((n_pairs, 8))
+        hi_np = np.zeros((n_pairs, bins))
+        t0 = time.perf_counter()
+        prop.propagate_into(b, ro, hits_np, st_np, hi_np, plain=True)
+        t_ph = time.perf_counter() - t0
+        ph = photons_local[0]
+        plain = {"kernel_photons_per_s": reduce(ph, SUM) / reduce(t_pk, MAX),
+                 "host_api_photons_per_s": reduce(ph, SUM) / reduce(t_ph, MAX),
+                 "launches_per_pass": 3 * n_pairs}
+        plain["batched_over_plain_kernel"] = value / plain["kernel_photons_per_s"]
+        plain["batched_over_plain_host_api"] = value / plain["host_api_photons_per_s"]
+
+    # e2e: the C-ABI host-buffer call, pinned host memory, copies inside the timing
+    pin_pairs = [torch.from_numpy(b.view(np.uint8).copy()).pin_memory().numpy().view(pp.PAIR_DTYPE)
+                 for b in batches]
+    pin_hits = torch.empty(cap * 64, dtype=torch.uint8).pin_memory().numpy().view(pp.HIT_DTYPE)
+    pin_stats = torch.empty(n_pairs * 8, dtype=torch.float64).pin_memory().numpy().reshape(n_pairs, 8)
+    pin_hist = torch.empty(n_pairs * bins, dtype=torch.float64).pin_memory().numpy().reshape(n_pairs, bins)
+    prop.propagate_into(pin_pairs[0], ro, pin_hits, pin_stats, pin_hist)
+    barrier()
+    e2e_t = 0.0
+    d2h = 0
+    for k in range(K):
+        t0 = time.perf_counter()
+        nh, _ = prop.propagate_into(pin_pairs[W + k], ro, pin_hits, pin_stats, pin_hist)
+        e2e_t += time.perf_counter() - t0
+        d2h += 32 + min(nh, cap) * 64 + n_pairs * 8 * 8 + n_pairs * bins * 8
+    e2e_value = photons_all / reduce(e2e_t, MAX)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(batches[W], args.cpu_seconds, RUN_KW)
+
+    lat = sorted(step_ms)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": reduce(t_local, MAX) * 1e3 / K, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "pairs": n_pairs, "photons_per_step_per_gpu": photons_local[0],
+                   "mode": "physical", "histogram": "1000 x 1 ns FP64 per pair",
+                   "l2": "flushed between steps (256 MiB write, outside the per-step events)",
+                   "launch": {"block": ro.block_size, "blocks_per_sm": ro.blocks_per_sm,
+                              "chunk_photons": ro.chunk_photons, "autotuned": tune is not None},
+                   "timing": "CUDA events per step on the launch stream, summed; max over ranks",
+                   "parallelism": f"{world} independent ranks (weak scaling, no collective)"},
+        "latency_ms": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                       "what": "device time of one 4096-pair batch solve"},
+        "roofline": {"bound": "mufu", "achieved": a_mufu / 1e9, "peak": peaks["mufu_ops"] / 1e9,
+                     "unit": "Gop/s", "frac": f_mufu, "traffic": None,
+                     "peak_source": "measured live: ex2.approx dependent chains over every SM (pp_measure_peaks)",
+                     "fp32": {"achieved": a_fp32 / 1e9, "peak": peaks["fp32_ops"] / 1e9, "frac": f_fp32},
+                     "int": {"achieved": a_int / 1e9, "peak": peaks["int_ops"] / 1e9,
+                             "frac": a_int / peaks["int_ops"]},
+                     "photon_steps_per_s": steps_total / t_local,
+                     "steps_per_photon": steps_total / max(sum(photons_local), 1),
+                     "hbm": {"achieved_gbs": hits_local * 64 / t_local / 1e9, "peak_gbs": 6551.0,
+                             "what": "hit write-back"}},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n_pairs * 80,
+                "d2h_bytes_per_step": int(d2h / K)},
+        "plain": plain,
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches,
+        "wall_s": wall,
+        "hits_per_step": hits_local / K,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    prop.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,263 @@
+/*
+ * photonprop_b200 — B200-native (sm_100a) photon propagation for PhotonProp.jl.
+ *
+ * C ABI of libphotonprop_b200.so.  Plain C types only (no CUDA, no torch in
+ * the signatures) so that Julia can bind every entry point with `ccall` and
+ * isbits mirror structs; the Python host package binds it with ctypes.
+ *
+ * Conventions
+ *  - Every fallible call returns pp_status; no exception crosses the ABI.
+ *    pp_last_error(ctx) returns a message for the last failure on ctx.
+ *  - The caller owns every host buffer it passes in; the library owns its
+ *    device buffers and the device-resident physics tables of a context.
+ *  - A context is bound to one device; calls on one context are serialised
+ *    by an internal mutex.  *_device entry points take device pointers and a
+ *    cudaStream_t (as void*) and return without synchronising.
+ *  - Units: metres, nanoseconds, nanometres.
+ *
+ * Citations are to the reference PhotonProp.jl (file:line).
+ */
+#ifndef PHOTONPROP_B200_H
+#define PHOTONPROP_B200_H
+
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define PP_API __attribute__((visibility("default")))
+#else
+#define PP_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PP_ABI_VERSION 1
+
+typedef enum {
+  PP_OK = 0,
+  PP_ERR_ARG = 1,      /* invalid argument; the reference throws ArgumentError */
+  PP_ERR_OOM = 2,      /* device or host allocation failed */
+  PP_ERR_OVERFLOW = 3, /* more hits than hit_capacity: the first hit_capacity
+                          are returned, *n_hits holds the true count */
+  PP_ERR_TIMEOUT = 4,  /* a bounded wait ran out (serving loop) */
+  PP_ERR_CUDA = 5,     /* a CUDA runtime call failed */
+  PP_ERR_STATE = 6,    /* call not valid in the object's current state */
+  PP_ERR_BUSY = 7      /* admission refused: no slot or memory free now */
+} pp_status;
+
+enum { PP_MODE_COMPAT = 0, PP_MODE_PHYSICAL = 1 };
+enum { PP_EMITTER_ISOTROPIC = 0, PP_EMITTER_CHERENKOV_CONE = 1 };
+enum { PP_SPECTRUM_CHERENKOV = 0, PP_SPECTRUM_MONOCHROMATIC = 1 };
+enum {
+  PP_OPT_PMT_WEIGHT = 1u, /* multiply hit weights by the PMT acceptance */
+  PP_OPT_NORMALIZE = 2u,  /* divide each pair's histogram by its photon count */
+  PP_OPT_NO_HITS = 4u     /* accumulate statistics only; write no hit records */
+};
+
+#define PP_MAX_KNOTS 64
+#define PP_MAX_ABS 32
+#define PP_MAX_PMT 256
+#define PP_STATS 8 /* per pair: hits, sum w, sum w^2, sum w t, sum w t^2,
+                      sum w ln t, photons, reserved */
+
+/* WaterProperties, src/medium.jl:23-50 (permille, atm, degC, ppm, ppm,
+ * g/cm^2) plus its absorption-length table, src/medium.jl:243-251
+ * (n_abs == 0 selects the reference's 6-knot table). */
+typedef struct {
+  double salinity;
+  double pressure;
+  double temperature;
+  double vol_conc_small_part;
+  double vol_conc_large_part;
+  double radiation_length;
+  int32_t n_abs;
+  int32_t pad;
+  double abs_wl[PP_MAX_ABS];
+  double abs_len[PP_MAX_ABS];
+} pp_medium_desc;
+
+/* CherenkovSpectrum(wl_range, interp_steps, medium), src/spectrum.jl:90-103,
+ * or Monochromatic(wavelength), src/spectrum.jl:14-16 (wl_min). */
+typedef struct {
+  int32_t kind;
+  int32_t n_knots;
+  double wl_min;
+  double wl_max;
+} pp_spectrum_desc;
+
+/* PMTWavelengthAcceptance table, src/detection.jl:18-33 (sorted by
+ * wavelength; n == 0 means acceptance 1). */
+typedef struct {
+  int32_t n;
+  int32_t pad;
+  double wavelength[PP_MAX_PMT];
+  double acceptance[PP_MAX_PMT];
+} pp_pmt_desc;
+
+/* One source-target pair: PhotonSource (src/emission.jl:102-109) plus
+ * DetectionSphere (src/detection.jl:10-15).  80 bytes. */
+typedef struct {
+  float pos[3];      /* emitter position (track start for a cone emitter) */
+  float t0;          /* emission time, ns */
+  float dir[3];      /* track direction of a cone emitter (unit) */
+  float track_len;   /* track length, m (cone emitter) */
+  float target[3];   /* sphere centre */
+  float radius;      /* sphere radius */
+  int64_t n_photons; /* photons to propagate */
+  uint64_t seed;     /* Philox key; the stream depends only on (seed, photon) */
+  int32_t emitter;   /* PP_EMITTER_* */
+  int32_t reserved[3];
+} pp_pair;
+
+/* Run options.  pp_default_opts fills the defaults of a mode. */
+typedef struct {
+  int32_t mode;       /* PP_MODE_COMPAT reproduces the reference arithmetic,
+                         PP_MODE_PHYSICAL the physical model */
+  int32_t max_steps;  /* compat: 10 (src/photon_prop_cuda.jl:319) */
+  float g;            /* Henyey-Greenstein asymmetry (reference: 0.99, :229) */
+  float t_max;        /* physical mode: photons end at this arrival time, ns */
+  float hist_t0;      /* arrival-time histogram origin, ns */
+  float hist_bin_width;
+  int32_t hist_bins;  /* 0: no histogram */
+  uint32_t flags;     /* PP_OPT_* */
+  int32_t block_size; /* launch tuning; 0 = autotuned/default */
+  int32_t blocks_per_sm;
+  int32_t chunk_photons;
+  int32_t reserved;
+} pp_run_opts;
+
+/* One detected photon.  64 bytes, written with four 16-byte stores. */
+typedef struct {
+  float pos[3];     /* hit position on the sphere */
+  float time;       /* arrival time, ns */
+  float dir0[3];    /* emission direction (reference output, :370) */
+  float weight;     /* absorption weight x PMT acceptance (if enabled) */
+  float dir[3];     /* arrival direction */
+  float wavelength; /* nm */
+  float dist;       /* path length, m */
+  uint32_t pair;    /* index of the pair in the call */
+  uint64_t photon;  /* photon index within the pair */
+} pp_hit;
+
+typedef struct pp_ctx pp_ctx;
+
+/* ---- library ------------------------------------------------------------ */
+PP_API int pp_abi_version(void);
+PP_API const char* pp_version(void);
+/* Kernels this process has launched through the library (all contexts). */
+PP_API uint64_t pp_launch_count(void);
+/* splitmix64 of (global_seed, index): the per-pair seed of a batch. */
+PP_API uint64_t pp_pair_seed(uint64_t global_seed, uint64_t index);
+
+/* ---- host physics (FP64; the reference's Medium/Spectral functions) ----- */
+/* get_refractive_index, src/medium.jl:125-158,179-183 */
+PP_API double pp_refractive_index(const pp_medium_desc* m, double wavelength_nm);
+/* group index n - lambda dn/dlambda of the same model (no reference counterpart) */
+PP_API double pp_group_index(const pp_medium_desc* m, double wavelength_nm);
+/* get_scattering_length, src/medium.jl:201-235 */
+PP_API double pp_scattering_length(const pp_medium_desc* m, double wavelength_nm);
+/* get_absorption_length, src/medium.jl:243-251 */
+PP_API double pp_absorption_length(const pp_medium_desc* m, double wavelength_nm);
+/* p_one_pmt_acc, src/detection.jl:27-33 */
+PP_API double pp_pmt_acceptance(const pp_pmt_desc* p, double wavelength_nm);
+/* CherenkovSpectrum(...).knots, src/spectrum.jl:54-70,77-82,96-101 */
+PP_API pp_status pp_cherenkov_knots(const pp_medium_desc* m, double wl_min, double wl_max,
+                             int32_t n_knots, double* knots_out);
+/* Fills the defaults of a mode: compat = 10 steps, g 0.99, no time window;
+ * physical = g 0.95, t_max 500 ns, 500 x 1 ns bins. */
+PP_API pp_status pp_default_opts(int32_t mode, pp_run_opts* out);
+
+/* ---- context ------------------------------------------------------------ */
+/* Builds the device-resident tables (spectrum knots, absorption and PMT
+ * tables, medium coefficients) on `device`.  pmt may be NULL. */
+PP_API pp_status pp_create(pp_ctx** out, int device, const pp_medium_desc* medium,
+                    const pp_spectrum_desc* spectrum, const pp_pmt_desc* pmt);
+PP_API void pp_destroy(pp_ctx* ctx);
+PP_API const char* pp_last_error(const pp_ctx* ctx);
+PP_API int pp_device(const pp_ctx* ctx);
+/* The float spectrum knots resident on the device. */
+PP_API pp_status pp_get_knots(const pp_ctx* ctx, float* out, int32_t cap, int32_t* n);
+
+/* ---- hot path ------------------------------------------------------------ */
+/* Batched persistent kernel over all pairs (device work queue of photon
+ * chunks), host buffers, synchronous.  Replaces propagate_distance
+ * (src/photon_prop_cuda.jl:588-644) for any number of source-target pairs.
+ * hits: hit_capacity records (may be NULL with capacity 0); stats:
+ * n_pairs x PP_STATS doubles; hist: n_pairs x hist_bins doubles (NULL if
+ * hist_bins == 0).  *n_hits receives the total hit count. */
+PP_API pp_status pp_propagate(pp_ctx* ctx, const pp_pair* pairs, int64_t n_pairs,
+                       const pp_run_opts* opts, pp_hit* hits, int64_t hit_capacity,
+                       int64_t* n_hits, double* stats, double* hist);
+
+/* Same results, one kernel launch per pair with a host synchronisation and
+ * copy-back after each, as propagate_distance does per distance
+ * (src/modelling.jl:96-99). */
+PP_API pp_status pp_propagate_plain(pp_ctx* ctx, const pp_pair* pairs, int64_t n_pairs,
+                             const pp_run_opts* opts, pp_hit* hits, int64_t hit_capacity,
+                             int64_t* n_hits, double* stats, double* hist);
+
+/* Device-buffer, asynchronous form of pp_propagate on `stream` (a
+ * cudaStream_t; NULL = legacy default stream).  counters: 4 uint64 on the
+ * device, [0] = total hits, [1] = photon steps taken, [2] = status bits
+ * (1 = hit overflow), [3] reserved; they are reset by the call.  The work
+ * queue lives in context-owned device scratch memory.  Repeated calls with
+ * the same shapes and buffers replay a captured CUDA graph. */
+PP_API pp_status pp_propagate_device(pp_ctx* ctx, const pp_pair* d_pairs, int64_t n_pairs,
+                              const pp_run_opts* opts, pp_hit* d_hits, int64_t hit_capacity,
+                              uint64_t* d_counters, double* d_stats, double* d_hist,
+                              void* stream);
+
+/* Device-buffer form of the plain kernel for one pair (no graph). */
+PP_API pp_status pp_propagate_plain_device(pp_ctx* ctx, const pp_pair* d_pair, const pp_pair* h_pair,
+                                    int64_t pair_index, const pp_run_opts* opts, pp_hit* d_hits,
+                                    int64_t hit_capacity, uint64_t* d_counters, double* d_stats,
+                                    double* d_hist, void* stream);
+
+/* Kernel-level drop-in for cuda_propagate_photons!
+ * (src/photon_prop_cuda.jl:262-386) with the reference's output layout:
+ * per-block hit stacks of stack_len entries in SoA device arrays
+ * (positions/directions: 3 floats per entry), 1-based per-block stack
+ * pointers (0 = empty block; the index of the block's last hit) and the
+ * number of photons simulated.  Each of n_blocks x threads threads
+ * simulates cld(n_photons, n_blocks*threads) photons and a block stops when
+ * its stack is nearly full, as in the reference.  source_target gives the
+ * source and sphere; opts the physics mode (compat reproduces the
+ * reference). */
+PP_API pp_status pp_cuda_propagate_photons(pp_ctx* ctx, float* d_out_positions,
+                                    float* d_out_directions, float* d_out_wavelengths,
+                                    float* d_out_dist_travelled,
+                                    int32_t* d_out_stack_pointers,
+                                    int64_t* d_out_n_ph_simulated, int32_t stack_len,
+                                    int32_t n_blocks, int32_t threads,
+                                    const pp_pair* source_target, const pp_run_opts* opts,
+                                    void* stream);
+
+/* ---- tuning and diagnostics ---------------------------------------------- */
+/* Times the batched kernel over (block size, blocks per SM, chunk) on a
+ * sample of `pairs` and stores the best in the context (and in the cache
+ * file at cache_path if not NULL).  best_out may be NULL. */
+PP_API pp_status pp_autotune(pp_ctx* ctx, const pp_pair* pairs, int64_t n_pairs,
+                      const pp_run_opts* opts, const char* cache_path,
+                      pp_run_opts* best_out, double* best_photons_per_s);
+
+/* Evaluates a device helper on n inputs (unit tests of the device code, the
+ * counterpart of the reference's apply_rot test kernel,
+ * src/tests/test_photon_prob.jl:32-35).  op: 0 philox words (in: 6 per item
+ * ctr0..3,key0..1 as doubles; out: 4), 1 uniform (in: word; out: 1),
+ * 2 HG cos theta (in: g,u), 3 rotate_to_axis (in: old[3],new[3]; out: 3),
+ * 4 update_position (in: pos[3],dir[3],step; out: 3), 5 equidistant
+ * interpolation of the context's knots (in: u), 6 refractive index,
+ * 7 group index, 8 scattering length, 9 absorption length, 10 PMT
+ * acceptance (in: wavelength). */
+PP_API pp_status pp_device_eval(pp_ctx* ctx, int32_t op, const double* in, double* out, int64_t n);
+
+/* Measures this device's FP32 FMA and MUFU (transcendental) issue peaks with
+ * dependent-chain microbenchmarks over every SM: operations per second. */
+PP_API pp_status pp_measure_peaks(int device, double* fp32_ops_per_s, double* mufu_ops_per_s,
+                           double* int_ops_per_s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

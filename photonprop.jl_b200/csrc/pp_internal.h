@@ -1,0 +1,59 @@
+// Internal interfaces between the C-ABI layer (pp_capi.cu) and the kernels
+// (pp_kernels.cu) / host physics (pp_host_physics.cpp).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+
+#include "photonprop_b200.h"
+
+namespace pp {
+
+// Everything one launch of the propagation kernels reads or writes.
+struct LaunchArgs {
+  const pp_pair* pairs;
+  int64_t n_pairs;
+  unsigned long long* chunk_offsets;  // [n_pairs + 1] scratch
+  unsigned long long* queue;          // [1] scratch
+  uint32_t chunk;
+  pp_hit* hits;
+  unsigned long long hit_cap;
+  unsigned long long* counters;  // [4]
+  double* stats;
+  double* hist;
+  const void* tables;  // device DevTables
+  pp_run_opts opts;
+};
+
+void count_launches(uint64_t n);
+
+size_t dev_tables_size();
+// coeffs: a01, a2, a3, a4, sca0, sca1, sca2 (+ unused)
+void fill_dev_tables(void* host_tables, const double coeffs[11], const float* knots, int n_knots,
+                     const float* abs_wl, const float* abs_len, int n_abs, const float* pmt_wl,
+                     const float* pmt_acc, int n_pmt);
+void get_dev_knots(const void* host_tables, float* out, int* n);
+
+cudaError_t launch_chunk_scan(const LaunchArgs& a, cudaStream_t s);
+cudaError_t launch_reset_counters(unsigned long long* counters, cudaStream_t s);
+cudaError_t launch_batched(const LaunchArgs& a, int grid, int block, cudaStream_t s);
+cudaError_t launch_plain(const LaunchArgs& a, const pp_pair* d_pair, int pair_index, int grid, int block,
+                         cudaStream_t s);
+cudaError_t launch_stacks(const LaunchArgs& a, const pp_pair* d_pair, float* pos, float* dir, float* wl,
+                          float* dist, int32_t* sp, int64_t* nsim, int stack_len, int grid, int block,
+                          long long per_thread, cudaStream_t s);
+cudaError_t launch_finalize(const pp_pair* pairs, int64_t n, double* stats, double* hist, int bins, int normalize,
+                            int sm_count, cudaStream_t s);
+cudaError_t launch_eval(int op, const double* in, double* out, int64_t n, const void* tables, cudaStream_t s);
+int batched_max_blocks_per_sm(int mode, int block);
+int plain_max_blocks_per_sm(int mode, int block);
+cudaError_t run_peaks(int sm_count, double* fp32, double* mufu, double* iops);
+
+// host physics (pp_host_physics.cpp)
+void medium_coeffs(const pp_medium_desc* m, double out[11]);
+void default_abs_table(double* wl, double* len, int* n);
+
+}  // namespace pp

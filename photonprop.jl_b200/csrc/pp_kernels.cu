@@ -1,0 +1,580 @@
+// Kernels of the photon-propagation hot path (sm_100a).
+//
+//  batched_kernel  persistent: each warp pulls photon chunks of any pair from a
+//                  device work queue and refills a lane as soon as its photon
+//                  ends, so lanes never idle behind a long-lived photon and
+//                  thousands of uneven pairs run in one launch.
+//  plain_kernel    one pair per launch, one photon per thread at a time
+//                  (grid-stride), the straightforward port of the reference's
+//                  thread loop (src/photon_prop_cuda.jl:301-380).
+//  stacks_kernel   cuda_propagate_photons! with the reference's output layout
+//                  (per-block hit stacks, src/photon_prop_cuda.jl:262-386).
+//  chunk_scan_kernel / finalize_kernel   work-queue set-up and FP64
+//                  normalisation.
+//  eval_kernel     device helpers on test inputs.
+//  peak kernels    FP32 / MUFU / INT issue microbenchmarks for the roofline.
+#include <cooperative_groups.h>
+#include <cuda_runtime.h>
+
+#include "pp_device.cuh"
+#include "pp_internal.h"
+
+namespace ppd {
+
+// ---------------------------------------------------------------------------
+// Batched persistent kernel.
+template <int MODE>
+__global__ void __launch_bounds__(512) batched_kernel(const RunParams R) {
+  __shared__ __align__(16) DevTables T;
+  stage_tables(T, R.tables);
+  __syncthreads();
+
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned lt_mask = (1u << lane) - 1u;
+  const unsigned long long total_chunks = R.chunk_offsets[R.n_pairs];
+
+  // warp-uniform work state
+  unsigned long long c_next = 0, c_end = 0;
+  int c_pair = 0;
+  bool warp_done = false;
+
+  // lane state
+  bool alive = false;
+  bool fresh = false;
+  int pair = 0;
+  Photon s;
+  s.id = 0;
+  PairCtx c;
+  c.index = 0;
+  unsigned steps = 0;
+
+  for (;;) {
+    unsigned need = __ballot_sync(kFull, !alive);
+    fresh = false;
+    while (need != 0u && !warp_done) {
+      if (c_next >= c_end) {
+        unsigned long long cid = 0, start = 0, end = 0;
+        int p = 0;
+        if (lane == 0) {
+          cid = atomicAdd(R.queue, 1ull);
+          if (cid < total_chunks) {
+            int lo = 0, hi = (int)R.n_pairs - 1;  // last pair with offset <= cid
+            while (lo < hi) {
+              const int mid = (lo + hi + 1) >> 1;
+              if (R.chunk_offsets[mid] <= cid) lo = mid; else hi = mid - 1;
+            }
+            p = lo;
+            start = (cid - R.chunk_offsets[p]) * (unsigned long long)R.chunk;
+            const unsigned long long n = (unsigned long long)R.pairs[p].n_photons;
+            end = min(start + (unsigned long long)R.chunk, n);
+          }
+        }
+        cid = __shfl_sync(kFull, cid, 0);
+        if (cid >= total_chunks) {
+          warp_done = true;
+          break;
+        }
+        c_pair = __shfl_sync(kFull, p, 0);
+        c_next = __shfl_sync(kFull, start, 0);
+        c_end = __shfl_sync(kFull, end, 0);
+      }
+      const unsigned avail = (unsigned)min(c_end - c_next, 32ull);
+      const unsigned rank = __popc(need & lt_mask);
+      if (!alive && rank < avail) {
+        pair = c_pair;
+        s.id = c_next + rank;
+        alive = true;
+        fresh = true;
+      }
+      c_next += min((unsigned)__popc(need), avail);
+      need = __ballot_sync(kFull, !alive);
+    }
+    if (fresh) {
+      const pp_pair P = R.pairs[pair];
+      c = load_pair_ctx(P, pair);
+      start_photon<MODE>(T, P, c, R, s.id, s);
+    }
+    if (__ballot_sync(kFull, alive) == 0u) break;
+    bool hit = false;
+    if (alive) {
+      ++steps;
+      alive = step_photon<MODE>(R, c, s, hit);
+    }
+    if (__any_sync(kFull, hit)) {
+      if (hit) {
+        const pp_pair P = R.pairs[c.index];
+        const HitValues h = hit_values<MODE>(T, R, P, c, s);
+        record_hit(R, c, s, h, c.index);
+      }
+    }
+  }
+  // photon-step count for the roofline
+  unsigned long long st = steps;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) st += __shfl_xor_sync(kFull, st, o);
+  if (lane == 0) atomicAdd(R.counters + 1, st);
+}
+
+// ---------------------------------------------------------------------------
+// Plain kernel: one pair, photons id = gtid + i * stride.
+template <int MODE>
+__global__ void __launch_bounds__(512) plain_kernel(const RunParams R, const pp_pair* __restrict__ pair_ptr,
+                                                    int pair_index) {
+  __shared__ __align__(16) DevTables T;
+  stage_tables(T, R.tables);
+  __syncthreads();
+  const pp_pair P = *pair_ptr;
+  const PairCtx c = load_pair_ctx(P, pair_index);
+  const unsigned long long n = (unsigned long long)P.n_photons;
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  unsigned steps = 0;
+  for (unsigned long long id = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; id < n;
+       id += stride) {
+    Photon s;
+    start_photon<MODE>(T, P, c, R, id, s);
+    bool alive = true;
+    while (alive) {
+      bool hit = false;
+      ++steps;
+      alive = step_photon<MODE>(R, c, s, hit);
+      if (hit) {
+        const HitValues h = hit_values<MODE>(T, R, P, c, s);
+        record_hit(R, c, s, h, 0);
+      }
+    }
+  }
+  unsigned long long st = steps;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) st += __shfl_xor_sync(kFull, st, o);
+  if ((threadIdx.x & 31u) == 0) atomicAdd(R.counters + 1, st);
+}
+
+// ---------------------------------------------------------------------------
+// cuda_propagate_photons! layout (src/photon_prop_cuda.jl:262-386).  Photon
+// ids: thread g simulates ids g + i * (blocks * threads), i < per_thread.
+template <int MODE>
+__global__ void __launch_bounds__(1024) stacks_kernel(const RunParams R, const pp_pair* __restrict__ pair_ptr,
+                                                      float* __restrict__ out_pos, float* __restrict__ out_dir,
+                                                      float* __restrict__ out_wl, float* __restrict__ out_dist,
+                                                      int32_t* __restrict__ out_sp,
+                                                      long long* __restrict__ out_nsim, int stack_len,
+                                                      long long per_thread) {
+  __shared__ __align__(16) DevTables T;
+  __shared__ int cursor;
+  stage_tables(T, R.tables);
+  const int ix_offset = (int)blockIdx.x * stack_len + 1;  // 1-based, as in the reference
+  if (threadIdx.x == 0) cursor = ix_offset;
+  __syncthreads();
+  const pp_pair P = *pair_ptr;
+  const PairCtx c = load_pair_ctx(P, 0);
+  const int safe_margin = max(0, (int)blockDim.x - 32);
+  const unsigned long long G = (unsigned long long)gridDim.x * blockDim.x;
+  const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long n_sim = 0;
+  unsigned steps = 0;
+  for (long long i = 0; i < per_thread; ++i) {
+    if (*(volatile int*)&cursor > ix_offset + stack_len - safe_margin) break;
+    Photon s;
+    start_photon<MODE>(T, P, c, R, g + (unsigned long long)i * G, s);
+    bool alive = true;
+    while (alive) {
+      bool hit = false;
+      ++steps;
+      alive = step_photon<MODE>(R, c, s, hit);
+      if (hit) {
+        const Emission e = emit_photon<MODE>(T, P, s.id, c.k0, c.k1);
+        const int idx = atomicAdd(&cursor, 1);  // 1-based slot
+        if (idx < ix_offset + stack_len) {
+          const int j = idx - 1;
+          out_pos[3 * j + 0] = s.px;
+          out_pos[3 * j + 1] = s.py;
+          out_pos[3 * j + 2] = s.pz;
+          out_dir[3 * j + 0] = e.dx;
+          out_dir[3 * j + 1] = e.dy;
+          out_dir[3 * j + 2] = e.dz;
+          out_wl[j] = e.wl;
+          out_dist[j] = s.dist;
+          atomicMax(out_sp + blockIdx.x, idx);
+        } else {
+          atomicOr(R.counters + 2, 1ull);
+        }
+      }
+    }
+    ++n_sim;
+  }
+  atomicAdd(reinterpret_cast<unsigned long long*>(out_nsim), (unsigned long long)n_sim);
+  atomicAdd(R.counters + 1, (unsigned long long)steps);
+}
+
+// ---------------------------------------------------------------------------
+// Chunk offsets of the work queue: offsets[p] = sum_{q<p} ceil(N_q / chunk),
+// offsets[n] = total.  One block; also resets the queue and counters.
+__global__ void __launch_bounds__(1024) chunk_scan_kernel(const pp_pair* __restrict__ pairs, int64_t n,
+                                                          uint32_t chunk,
+                                                          unsigned long long* __restrict__ offsets,
+                                                          unsigned long long* __restrict__ queue,
+                                                          unsigned long long* __restrict__ counters) {
+  __shared__ unsigned long long warp_sums[32];
+  const int t = threadIdx.x;
+  const int64_t per = (n + blockDim.x - 1) / blockDim.x;
+  const int64_t b = (int64_t)t * per;
+  const int64_t e = min(b + per, n);
+  unsigned long long local = 0;
+  for (int64_t i = b; i < e; ++i) {
+    const long long np = pairs[i].n_photons;
+    local += np > 0 ? ((unsigned long long)np + chunk - 1) / chunk : 0ull;
+  }
+  // exclusive block scan of `local`
+  const unsigned lane = t & 31, warp = t >> 5;
+  unsigned long long incl = local;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long v = __shfl_up_sync(kFull, incl, o);
+    if ((int)lane >= o) incl += v;
+  }
+  if (lane == 31) warp_sums[warp] = incl;
+  __syncthreads();
+  if (warp == 0) {
+    unsigned long long w = (lane < (blockDim.x >> 5)) ? warp_sums[lane] : 0ull;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long v = __shfl_up_sync(kFull, w, o);
+      if ((int)lane >= o) w += v;
+    }
+    warp_sums[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  unsigned long long run = incl - local + (warp > 0 ? warp_sums[warp - 1] : 0ull);
+  for (int64_t i = b; i < e; ++i) {
+    offsets[i] = run;
+    const long long np = pairs[i].n_photons;
+    run += np > 0 ? ((unsigned long long)np + chunk - 1) / chunk : 0ull;
+  }
+  if (t == (int)blockDim.x - 1) offsets[n] = warp_sums[(blockDim.x >> 5) - 1];
+  if (t == 0) {
+    queue[0] = 0ull;
+    counters[0] = 0ull;
+    counters[1] = 0ull;
+    counters[2] = 0ull;
+    counters[3] = 0ull;
+  }
+}
+
+__global__ void reset_counters_kernel(unsigned long long* __restrict__ counters) {
+  if (threadIdx.x < 4) counters[threadIdx.x] = 0ull;
+}
+
+// stats[p][6] = photons; optionally hist[p][:] /= photons.
+__global__ void finalize_kernel(const pp_pair* __restrict__ pairs, int64_t n_pairs, double* __restrict__ stats,
+                                double* __restrict__ hist, int bins, int normalize) {
+  const int64_t total = n_pairs * (int64_t)(bins > 0 ? bins : 1);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t p = bins > 0 ? i / bins : i;
+    const double n = (double)pairs[p].n_photons;
+    if (bins <= 0 || i % bins == 0) stats[p * PP_STATS + 6] = n;
+    if (normalize && bins > 0 && n > 0) hist[i] /= n;
+  }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void eval_kernel(int op, const double* __restrict__ in, double* __restrict__ out, int64_t n,
+                            const DevTables* __restrict__ tables) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const DevTables& T = *tables;
+  switch (op) {
+    case 0: {
+      const double* a = in + 6 * i;
+      uint32_t c[4] = {(uint32_t)a[0], (uint32_t)a[1], (uint32_t)a[2], (uint32_t)a[3]};
+      philox4x32_10(c, (uint32_t)a[4], (uint32_t)a[5]);
+      for (int j = 0; j < 4; ++j) out[4 * i + j] = (double)c[j];
+      break;
+    }
+    case 1: out[i] = (double)u01((uint32_t)in[i]); break;
+    case 2: {
+      const float g = (float)in[2 * i];
+      HG h;
+      h.iso = (g == 0.f);
+      h.two_g = 2.f * g;
+      h.one_m_g = 1.f - g;
+      h.a = 1.f - g * g;
+      h.one_p_g2 = 1.f + g * g;
+      h.inv_2g = h.iso ? 0.f : 1.f / (2.f * g);
+      out[i] = (double)hg_costheta(h, (float)in[2 * i + 1]);
+      break;
+    }
+    case 3: {
+      const double* a = in + 6 * i;
+      float x, y, z;
+      rotate_to_axis((float)a[0], (float)a[1], (float)a[2], (float)a[3], (float)a[4], (float)a[5], x, y, z);
+      out[3 * i] = x;
+      out[3 * i + 1] = y;
+      out[3 * i + 2] = z;
+      break;
+    }
+    case 4: {
+      const double* a = in + 7 * i;
+      const float st = (float)a[6];
+      out[3 * i] = fmaf(st, (float)a[3], (float)a[0]);
+      out[3 * i + 1] = fmaf(st, (float)a[4], (float)a[1]);
+      out[3 * i + 2] = fmaf(st, (float)a[5], (float)a[2]);
+      break;
+    }
+    case 5: out[i] = (double)draw_wavelength(T, (float)in[i]); break;
+    case 6: out[i] = (double)phase_index(T, 1.f / (float)in[i]); break;
+    case 7: out[i] = (double)group_index(T, 1.f / (float)in[i]); break;
+    case 8: out[i] = (double)scattering_length(T, (float)in[i]); break;
+    case 9: out[i] = (double)interp_sorted((float)in[i], T.abs_wl, T.abs_len, T.n_abs); break;
+    case 10:
+      out[i] = T.n_pmt > 0 ? (double)interp_sorted((float)in[i], T.pmt_wl, T.pmt_acc, T.n_pmt) : 1.0;
+      break;
+    default: out[i] = 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Issue-rate microbenchmarks: 8 independent dependent chains per thread.
+__global__ void peak_fma_kernel(float* out, int iters, float a, float b) {
+  float x[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) x[j] = (float)(threadIdx.x + j);
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = fmaf(x[j], a, b);
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += x[j];
+  if (s == 1.2345f) out[0] = s;
+}
+
+__global__ void peak_mufu_kernel(float* out, int iters) {
+  float x[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) x[j] = 0.5f + 0.01f * (float)(threadIdx.x & 7) + 0.001f * j;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = ex2(x[j] * -0.5f);  // ex2 of a value in (0,1): stays in (0,1)
+  }
+  float s = 0.f;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s += x[j];
+  if (s == 1.2345f) out[0] = s;
+}
+
+__global__ void peak_int_kernel(unsigned* out, int iters) {
+  unsigned x[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) x[j] = threadIdx.x * 2654435761u + j;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) x[j] = x[j] * 0x9E3779B9u + 0x7F4A7C15u;  // IMAD
+  }
+  unsigned s = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) s ^= x[j];
+  if (s == 12345u) out[0] = s;
+}
+
+}  // namespace ppd
+
+// ---------------------------------------------------------------------------
+// Launch helpers (host).
+namespace pp {
+
+static __host__ ppd::RunParams to_params(const LaunchArgs& a) {
+  ppd::RunParams R;
+  R.pairs = a.pairs;
+  R.n_pairs = a.n_pairs;
+  R.chunk_offsets = a.chunk_offsets;
+  R.queue = a.queue;
+  R.chunk = a.chunk;
+  R.pair_base = 0;
+  R.hits = a.hits;
+  R.hit_cap = a.hit_cap;
+  R.counters = a.counters;
+  R.stats = a.stats;
+  R.hist = a.hist;
+  R.tables = reinterpret_cast<const ppd::DevTables*>(a.tables);
+  R.max_steps = a.opts.max_steps;
+  R.t_max = a.opts.t_max;
+  R.hist_t0 = a.opts.hist_t0;
+  R.inv_bin_width = a.opts.hist_bin_width > 0.f ? 1.f / a.opts.hist_bin_width : 0.f;
+  R.hist_bins = a.opts.hist_bins;
+  R.flags = a.opts.flags;
+  const float g = a.opts.g;
+  R.hg.iso = (g == 0.f);
+  R.hg.two_g = 2.f * g;
+  R.hg.one_m_g = 1.f - g;
+  R.hg.a = 1.f - g * g;
+  R.hg.one_p_g2 = 1.f + g * g;
+  R.hg.inv_2g = R.hg.iso ? 0.f : 1.f / (2.f * g);
+  return R;
+}
+
+size_t dev_tables_size() { return sizeof(ppd::DevTables); }
+
+void fill_dev_tables(void* host_tables, const double coeffs[11], const float* knots, int n_knots,
+                     const float* abs_wl, const float* abs_len, int n_abs, const float* pmt_wl,
+                     const float* pmt_acc, int n_pmt) {
+  ppd::DevTables* t = reinterpret_cast<ppd::DevTables*>(host_tables);
+  memset(t, 0, sizeof(*t));
+  t->a01 = (float)coeffs[0];
+  t->a2 = (float)coeffs[1];
+  t->a3 = (float)coeffs[2];
+  t->a4 = (float)coeffs[3];
+  t->g01 = (float)coeffs[0];
+  t->g2 = (float)(2.0 * coeffs[1]);
+  t->g3 = (float)(3.0 * coeffs[2]);
+  t->g4 = (float)(4.0 * coeffs[3]);
+  t->sca0 = (float)coeffs[4];
+  t->sca1 = (float)coeffs[5];
+  t->sca2 = (float)coeffs[6];
+  t->n_knots = n_knots;
+  for (int i = 0; i < n_knots; ++i) t->knots[i] = knots[i];
+  t->n_abs = n_abs;
+  for (int i = 0; i < n_abs; ++i) {
+    t->abs_wl[i] = abs_wl[i];
+    t->abs_len[i] = abs_len[i];
+  }
+  t->n_pmt = n_pmt;
+  for (int i = 0; i < n_pmt; ++i) {
+    t->pmt_wl[i] = pmt_wl[i];
+    t->pmt_acc[i] = pmt_acc[i];
+  }
+}
+
+void get_dev_knots(const void* host_tables, float* out, int* n) {
+  const ppd::DevTables* t = reinterpret_cast<const ppd::DevTables*>(host_tables);
+  *n = t->n_knots;
+  for (int i = 0; i < t->n_knots; ++i) out[i] = t->knots[i];
+}
+
+cudaError_t launch_chunk_scan(const LaunchArgs& a, cudaStream_t s) {
+  ppd::chunk_scan_kernel<<<1, 1024, 0, s>>>(a.pairs, a.n_pairs, a.chunk, a.chunk_offsets, a.queue, a.counters);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_reset_counters(unsigned long long* counters, cudaStream_t s) {
+  ppd::reset_counters_kernel<<<1, 32, 0, s>>>(counters);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batched(const LaunchArgs& a, int grid, int block, cudaStream_t s) {
+  const ppd::RunParams R = to_params(a);
+  if (a.opts.mode == PP_MODE_COMPAT)
+    ppd::batched_kernel<ppd::kCompat><<<grid, block, 0, s>>>(R);
+  else
+    ppd::batched_kernel<ppd::kPhysical><<<grid, block, 0, s>>>(R);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plain(const LaunchArgs& a, const pp_pair* d_pair, int pair_index, int grid, int block,
+                         cudaStream_t s) {
+  const ppd::RunParams R = to_params(a);
+  if (a.opts.mode == PP_MODE_COMPAT)
+    ppd::plain_kernel<ppd::kCompat><<<grid, block, 0, s>>>(R, d_pair, pair_index);
+  else
+    ppd::plain_kernel<ppd::kPhysical><<<grid, block, 0, s>>>(R, d_pair, pair_index);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stacks(const LaunchArgs& a, const pp_pair* d_pair, float* pos, float* dir, float* wl,
+                          float* dist, int32_t* sp, int64_t* nsim, int stack_len, int grid, int block,
+                          long long per_thread, cudaStream_t s) {
+  const ppd::RunParams R = to_params(a);
+  if (a.opts.mode == PP_MODE_COMPAT)
+    ppd::stacks_kernel<ppd::kCompat><<<grid, block, 0, s>>>(R, d_pair, pos, dir, wl, dist, sp,
+                                                            reinterpret_cast<long long*>(nsim), stack_len,
+                                                            per_thread);
+  else
+    ppd::stacks_kernel<ppd::kPhysical><<<grid, block, 0, s>>>(R, d_pair, pos, dir, wl, dist, sp,
+                                                              reinterpret_cast<long long*>(nsim), stack_len,
+                                                              per_thread);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_finalize(const pp_pair* pairs, int64_t n, double* stats, double* hist, int bins, int normalize,
+                            int sm_count, cudaStream_t s) {
+  const int64_t total = n * (int64_t)(bins > 0 ? bins : 1);
+  int grid = (int)std::min<int64_t>((total + 255) / 256, (int64_t)sm_count * 8);
+  if (grid < 1) grid = 1;
+  ppd::finalize_kernel<<<grid, 256, 0, s>>>(pairs, n, stats, hist, bins, normalize);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eval(int op, const double* in, double* out, int64_t n, const void* tables, cudaStream_t s) {
+  const int grid = (int)((n + 127) / 128);
+  ppd::eval_kernel<<<grid, 128, 0, s>>>(op, in, out, n, reinterpret_cast<const ppd::DevTables*>(tables));
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+int batched_max_blocks_per_sm(int mode, int block) {
+  int nb = 0;
+  if (mode == PP_MODE_COMPAT)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kCompat>, block, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical>, block, 0);
+  return nb;
+}
+
+int plain_max_blocks_per_sm(int mode, int block) {
+  int nb = 0;
+  if (mode == PP_MODE_COMPAT)
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::plain_kernel<ppd::kCompat>, block, 0);
+  else
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::plain_kernel<ppd::kPhysical>, block, 0);
+  return nb;
+}
+
+cudaError_t run_peaks(int sm_count, double* fp32, double* mufu, double* iops) {
+  float* dout = nullptr;
+  cudaError_t e = cudaMalloc(&dout, 64);
+  if (e != cudaSuccess) return e;
+  cudaEvent_t a, b;
+  cudaEventCreate(&a);
+  cudaEventCreate(&b);
+  const int block = 256, grid = sm_count * 8;
+  const double threads = (double)grid * block;
+  float ms = 0.f;
+  // warm-up
+  ppd::peak_fma_kernel<<<grid, block>>>(dout, 1000, 0.999f, 0.001f);
+  ppd::peak_mufu_kernel<<<grid, block>>>(dout, 100);
+  ppd::peak_int_kernel<<<grid, block>>>(reinterpret_cast<unsigned*>(dout), 100);
+  count_launches(3);
+  const int it_f = 20000, it_m = 4000, it_i = 10000;
+  cudaEventRecord(a);
+  ppd::peak_fma_kernel<<<grid, block>>>(dout, it_f, 0.999f, 0.001f);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  cudaEventElapsedTime(&ms, a, b);
+  *fp32 = threads * it_f * 8.0 / (ms * 1e-3);
+  cudaEventRecord(a);
+  ppd::peak_mufu_kernel<<<grid, block>>>(dout, it_m);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  cudaEventElapsedTime(&ms, a, b);
+  *mufu = threads * it_m * 8.0 / (ms * 1e-3);
+  cudaEventRecord(a);
+  ppd::peak_int_kernel<<<grid, block>>>(reinterpret_cast<unsigned*>(dout), it_i);
+  cudaEventRecord(b);
+  cudaEventSynchronize(b);
+  cudaEventElapsedTime(&ms, a, b);
+  *iops = threads * it_i * 8.0 / (ms * 1e-3);
+  count_launches(3);
+  e = cudaGetLastError();
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  cudaFree(dout);
+  return e;
+}
+
+}  // namespace pp

@@ -1,0 +1,36 @@
+"""photonprop_b200: B200-native photon propagation for PhotonProp.jl.
+
+Python host mirror of the reference's Julia API (Medium, Spectral, Emission,
+Detection and PhotonPropagationCuda modules) over the C ABI of
+libphotonprop_b200.so, whose CUDA kernels (sm_100a) do all propagation.
+"""
+from . import _lib
+from ._lib import EXPORTED, HIT_DTYPE, PAIR_DTYPE, PPError
+from .detection import DetectionSphere, PMTWavelengthAcceptance, p_one_pmt_acc, p_one_pmt_acc_5nm
+from .emission import (AngularEmissionProfile, CherenkovEmission, IsotropicEmission, PhotonSource,
+                       cherenkov_ang_dist)
+from .medium import (WaterProperties, get_absorption_length, get_group_index, get_refractive_index,
+                     get_scattering_length, make_cascadia_medium_properties, make_seawater)
+from .propagation import (PropagationResult, Propagator, RunOptions, cuda_propagate_photons_,
+                          initialize_photon_arrays, make_pair, pair_seed, process_output,
+                          propagate_distance)
+from .spectrum import CherenkovSpectrum, Monochromatic, Spectrum
+from . import batches
+
+
+def build(force=False):
+    from . import _build
+    return _build.build(force=force)
+
+
+def launch_count() -> int:
+    return int(_lib.load().pp_launch_count())
+
+
+def measure_peaks(device=0):
+    """FP32 FMA, MUFU and INT multiply-add issue peaks of the device (ops/s)."""
+    import ctypes
+    L = _lib.load()
+    f, m, i = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    _lib.check(L.pp_measure_peaks(device, ctypes.byref(f), ctypes.byref(m), ctypes.byref(i)))
+    return {"fp32_ops": f.value, "mufu_ops": m.value, "int_ops": i.value}

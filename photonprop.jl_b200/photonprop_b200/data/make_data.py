@@ -1,0 +1,34 @@
+"""Regenerates the package data tables from the reference checkout.
+
+pmt_acceptance.csv: the PMT quantum-efficiency curve of PhotonProp.jl
+(PMTAcc.csv, read at module load by src/detection.jl:31-33), unchanged
+values, written with a header.  pmt_acceptance_5nm.csv: the same curve
+linearly interpolated at 5 nm from 300 to 700 nm (81 entries), the
+tabulation the one-pair-per-launch cone workload uses.
+
+Usage: python make_data.py /path/to/PhotonProp.jl
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def main(ref):
+    d = np.loadtxt(os.path.join(ref, "PMTAcc.csv"), delimiter=",")
+    with open(os.path.join(HERE, "pmt_acceptance.csv"), "w") as f:
+        f.write("# wavelength_nm,acceptance  (PhotonProp.jl PMTAcc.csv)\n")
+        for wl, acc in d:
+            f.write(f"{float(wl)!r},{float(acc)!r}\n")
+    grid = np.arange(300.0, 700.0 + 0.5, 5.0)
+    acc5 = np.interp(grid, d[:, 0], d[:, 1])
+    with open(os.path.join(HERE, "pmt_acceptance_5nm.csv"), "w") as f:
+        f.write("# wavelength_nm,acceptance  (PMTAcc.csv interpolated at 5 nm, 300-700 nm)\n")
+        for wl, acc in zip(grid, acc5):
+            f.write(f"{float(wl)!r},{float(acc)!r}\n")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
