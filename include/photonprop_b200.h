@@ -253,9 +253,10 @@ PP_API pp_status pp_autotune(pp_ctx* ctx, const pp_pair* pairs, int64_t n_pairs,
 PP_API pp_status pp_device_eval(pp_ctx* ctx, int32_t op, const double* in, double* out, int64_t n);
 
 /* Measures this device's FP32 FMA and MUFU (transcendental) issue peaks with
- * dependent-chain microbenchmarks over every SM: operations per second. */
+ * independent dependent-chain microbenchmarks over every SM (operations per
+ * second) and its Philox4x32-10 block rate (blocks per second). */
 PP_API pp_status pp_measure_peaks(int device, double* fp32_ops_per_s, double* mufu_ops_per_s,
-                           double* int_ops_per_s);
+                           double* philox_blocks_per_s);
 
 #ifdef __cplusplus
 }

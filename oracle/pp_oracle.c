@@ -11,8 +11,9 @@
  *   - arrival time t = t_emit + dist * n_group(lambda) / c;
  *   - a photon ends when its next position would lie beyond the time window
  *     t_max, when it hits the sphere, or after max_steps steps.
- * Random numbers: Philox4x32-10 (Salmon et al., SC'11), key = the pair's
- * 64-bit seed, counter = (photon index lo, hi, block, 0).  Block 0 gives the
+ * Random numbers: Philox4x32-10 (Salmon et al., SC'11) under the fixed key
+ * (0x243F6A88, 0x85A308D3) with counter (seed lo, seed hi, photon lo,
+ * photon hi | block << 8) for a photon index below 2^40.  Block 0 gives the
  * emission draws (wavelength, polar angle or track position, azimuth), block
  * k+1 the draws of step k (step length, HG cos(theta), azimuth).
  */
@@ -26,6 +27,8 @@
 #endif
 
 #define ORC_C_VAC 0.299792458
+#define ORC_KEY0 0x243F6A88u /* fixed Philox key */
+#define ORC_KEY1 0x85A308D3u
 #define ORC_TWO_PI 6.283185307179586
 
 /* Philox4x32-10, Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
@@ -157,8 +160,9 @@ static void hb_push(hitbuf* b, const orc_hit* h) {
 }
 
 static void philox_block(uint64_t seed, int64_t photon, uint32_t block, double u[4]) {
-  uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-  uint32_t ctr[4] = {(uint32_t)(uint64_t)photon, (uint32_t)((uint64_t)photon >> 32), block, 0u};
+  uint32_t key[2] = {ORC_KEY0, ORC_KEY1};
+  uint32_t ctr[4] = {(uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)(uint64_t)photon,
+                     (uint32_t)((uint64_t)photon >> 32) | (block << 8)};
   uint32_t w[4];
   orc_philox4x32_10(ctr, key, w);
   for (int i = 0; i < 4; ++i) u[i] = orc_uniform(w[i]);

@@ -45,10 +45,13 @@ struct DevBuf {
   }
 };
 
-cudaError_t ensure(DevBuf& b, size_t bytes) {
+// Grows a context buffer.  *grew is set when the buffer moved, which
+// invalidates every cached graph (they hold raw pointers).
+cudaError_t ensure(DevBuf& b, size_t bytes, bool* grew) {
   if (bytes == 0) bytes = 16;
   if (b.bytes >= bytes) return cudaSuccess;
   b.release();
+  *grew = true;
   cudaError_t e = cudaMalloc(&b.p, bytes);
   if (e == cudaSuccess) b.bytes = bytes;
   return e;
@@ -74,6 +77,8 @@ struct GraphKey {
   const void* stats;
   const void* hist;
   const void* stream;
+  const void* offsets;
+  const void* queue;
   int grid, block;
   uint32_t chunk;
   pp_run_opts opts;
@@ -134,7 +139,8 @@ namespace {
 pp_status validate_opts(pp_ctx* c, const pp_run_opts* o) {
   if (!o) return c->fail(PP_ERR_ARG, "opts is NULL");
   if (o->mode != PP_MODE_COMPAT && o->mode != PP_MODE_PHYSICAL) return c->fail(PP_ERR_ARG, "unknown mode");
-  if (o->max_steps < 1) return c->fail(PP_ERR_ARG, "max_steps must be >= 1");
+  if (o->max_steps < 1 || o->max_steps > (1 << 24) - 2)
+    return c->fail(PP_ERR_ARG, "max_steps must be in [1, 2^24 - 2] (the step is part of the Philox counter)");
   if (!(std::fabs(o->g) < 1.f)) return c->fail(PP_ERR_ARG, "|g| must be < 1");
   if (o->hist_bins < 0) return c->fail(PP_ERR_ARG, "hist_bins must be >= 0");
   if (o->hist_bins > 0 && !(o->hist_bin_width > 0.f)) return c->fail(PP_ERR_ARG, "hist_bin_width must be > 0");
@@ -152,8 +158,8 @@ pp_status validate_pairs(pp_ctx* c, const pp_pair* p, int64_t n, int mode) {
   for (int64_t i = 0; i < n; ++i) {
     const pp_pair& q = p[i];
     char buf[160];
-    if (q.n_photons < 0) {
-      snprintf(buf, sizeof buf, "pair %lld: n_photons < 0", (long long)i);
+    if (q.n_photons < 0 || q.n_photons > (1ll << 40)) {
+      snprintf(buf, sizeof buf, "pair %lld: n_photons must be in [0, 2^40]", (long long)i);
       return c->fail(PP_ERR_ARG, buf);
     }
     if (!(q.radius > 0.f) || !std::isfinite(q.radius)) {
@@ -184,6 +190,7 @@ pp_status validate_pairs(pp_ctx* c, const pp_pair* p, int64_t n, int mode) {
 void resolve_launch(pp_ctx* c, const pp_run_opts& o, int& grid, int& block, uint32_t& chunk) {
   const int m = o.mode;
   block = o.block_size > 0 ? o.block_size : c->tuned_block[m];
+  if (block != 128) block = 256;  // the batched kernel exists for 4- and 8-warp blocks
   int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : c->tuned_bps[m];
   const int maxb = pp::batched_max_blocks_per_sm(m, block);
   if (bps <= 0 || bps > maxb) bps = maxb > 0 ? maxb : 1;
@@ -223,6 +230,8 @@ cudaError_t run_batched(pp_ctx* c, const pp::LaunchArgs& a, cudaStream_t s, bool
   k.stats = b.stats;
   k.hist = b.hist;
   k.stream = s;
+  k.offsets = b.chunk_offsets;
+  k.queue = b.queue;
   k.grid = grid;
   k.block = block;
   k.chunk = chunk;
@@ -275,6 +284,8 @@ pp::LaunchArgs base_args(pp_ctx* c, const pp_run_opts* o) {
   a.opts = *o;
   return a;
 }
+
+bool aligned(const void* p, uintptr_t a) { return ((uintptr_t)p % a) == 0; }
 
 pp_status alloc_fail(pp_ctx* c, cudaError_t e, const char* what) {
   if (e == cudaErrorMemoryAllocation) {
@@ -455,11 +466,16 @@ pp_status pp_propagate_device(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs
   if (n_pairs < 0 || n_pairs > (int64_t)INT32_MAX || (n_pairs > 0 && !d_pairs) || !d_counters || !d_stats ||
       (opts->hist_bins > 0 && !d_hist) || cap < 0 || (cap > 0 && !d_hits))
     return c->fail(PP_ERR_ARG, "pp_propagate_device: bad buffer arguments");
+  if (!aligned(d_pairs, 16) || !aligned(d_hits, 16) || !aligned(d_counters, 8) || !aligned(d_stats, 8) ||
+      !aligned(d_hist, 8))
+    return c->fail(PP_ERR_ARG, "pp_propagate_device: pairs/hits need 16-byte, counters/stats/hist 8-byte alignment");
   DeviceGuard guard(c->device);
   cudaError_t e;
-  if ((e = ensure(c->offsets, (size_t)(n_pairs + 1) * sizeof(unsigned long long))) ||
-      (e = ensure(c->queue, 64)))
+  bool grew = false;
+  if ((e = ensure(c->offsets, (size_t)(n_pairs + 1) * sizeof(unsigned long long), &grew)) ||
+      (e = ensure(c->queue, 64, &grew)))
     return alloc_fail(c, e, "work-queue scratch");
+  if (grew) c->drop_graphs();
   pp::LaunchArgs a = base_args(c, opts);
   a.pairs = d_pairs;
   a.n_pairs = n_pairs;
@@ -486,12 +502,14 @@ pp_status pp_propagate(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const p
   DeviceGuard guard(c->device);
   const int bins = opts->hist_bins;
   cudaError_t e;
-  if ((e = ensure(c->pairs, (size_t)n_pairs * sizeof(pp_pair))) ||
-      (e = ensure(c->hits, (size_t)cap * sizeof(pp_hit))) || (e = ensure(c->counters, 64)) ||
-      (e = ensure(c->stats, (size_t)n_pairs * PP_STATS * sizeof(double))) ||
-      (e = ensure(c->hist, (size_t)n_pairs * (size_t)(bins > 0 ? bins : 1) * sizeof(double))) ||
-      (e = ensure(c->offsets, (size_t)(n_pairs + 1) * sizeof(unsigned long long))) || (e = ensure(c->queue, 64)))
+  bool grew = false;
+  if ((e = ensure(c->pairs, (size_t)n_pairs * sizeof(pp_pair), &grew)) ||
+      (e = ensure(c->hits, (size_t)cap * sizeof(pp_hit), &grew)) || (e = ensure(c->counters, 64, &grew)) ||
+      (e = ensure(c->stats, (size_t)n_pairs * PP_STATS * sizeof(double), &grew)) ||
+      (e = ensure(c->hist, (size_t)n_pairs * (size_t)(bins > 0 ? bins : 1) * sizeof(double), &grew)) ||
+      (e = ensure(c->offsets, (size_t)(n_pairs + 1) * sizeof(unsigned long long), &grew)) || (e = ensure(c->queue, 64, &grew)))
     return alloc_fail(c, e, "pp_propagate buffers");
+  if (grew) c->drop_graphs();
   cudaStream_t s = c->stream;
   if (n_pairs > 0 &&
       (e = cudaMemcpyAsync(c->pairs.p, pairs, (size_t)n_pairs * sizeof(pp_pair), cudaMemcpyHostToDevice, s)))
@@ -539,6 +557,9 @@ pp_status pp_propagate_plain_device(pp_ctx* c, const pp_pair* d_pair, const pp_p
   if (!d_pair || !h_pair || !d_counters || !d_stats || (opts->hist_bins > 0 && !d_hist) || cap < 0 ||
       (cap > 0 && !d_hits) || pair_index < 0 || pair_index > (int64_t)INT32_MAX)
     return c->fail(PP_ERR_ARG, "pp_propagate_plain_device: bad arguments");
+  if (!aligned(d_pair, 16) || !aligned(d_hits, 16) || !aligned(d_counters, 8) || !aligned(d_stats, 8) ||
+      !aligned(d_hist, 8))
+    return c->fail(PP_ERR_ARG, "pp_propagate_plain_device: pair/hits need 16-byte, counters/stats/hist 8-byte alignment");
   if ((st = validate_pairs(c, h_pair, 1, opts->mode))) return st;
   DeviceGuard guard(c->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
@@ -580,11 +601,13 @@ pp_status pp_propagate_plain(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, c
     DeviceGuard guard(c->device);
     const int bins = opts->hist_bins;
     cudaError_t e;
-    if ((e = ensure(c->pairs, (size_t)n_pairs * sizeof(pp_pair))) ||
-        (e = ensure(c->hits, (size_t)cap * sizeof(pp_hit))) || (e = ensure(c->counters, 64)) ||
-        (e = ensure(c->stats, PP_STATS * sizeof(double))) ||
-        (e = ensure(c->hist, (size_t)(bins > 0 ? bins : 1) * sizeof(double))))
+    bool grew = false;
+    if ((e = ensure(c->pairs, (size_t)n_pairs * sizeof(pp_pair), &grew)) ||
+        (e = ensure(c->hits, (size_t)cap * sizeof(pp_hit), &grew)) || (e = ensure(c->counters, 64, &grew)) ||
+        (e = ensure(c->stats, PP_STATS * sizeof(double), &grew)) ||
+        (e = ensure(c->hist, (size_t)(bins > 0 ? bins : 1) * sizeof(double), &grew)))
       return alloc_fail(c, e, "pp_propagate_plain buffers");
+    if (grew) c->drop_graphs();
     if (n_pairs > 0 && (e = cudaMemcpyAsync(c->pairs.p, pairs, (size_t)n_pairs * sizeof(pp_pair),
                                             cudaMemcpyHostToDevice, c->stream)))
       return c->cuda_fail(e, "copy pairs");
@@ -636,14 +659,19 @@ pp_status pp_cuda_propagate_photons(pp_ctx* c, float* pos, float* dir, float* wl
   if (!pos || !dir || !wl || !dist || !sp || !nsim || !st_pair || stack_len < 1 || n_blocks < 1 || threads < 32 ||
       threads > 1024 || threads % 32)
     return c->fail(PP_ERR_ARG, "pp_cuda_propagate_photons: bad arguments");
+  if (!aligned(pos, 4) || !aligned(dir, 4) || !aligned(wl, 4) || !aligned(dist, 4) || !aligned(sp, 4) ||
+      !aligned(nsim, 8))
+    return c->fail(PP_ERR_ARG, "pp_cuda_propagate_photons: misaligned output array");
   if ((int64_t)stack_len * n_blocks > (int64_t)INT32_MAX)
     return c->fail(PP_ERR_ARG, "stack_len * n_blocks exceeds int32 indices");
   if ((st = validate_pairs(c, st_pair, 1, opts->mode))) return st;
   DeviceGuard guard(c->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   cudaError_t e;
-  if ((e = ensure(c->pairs, sizeof(pp_pair))) || (e = ensure(c->counters, 64)))
+  bool grew = false;
+  if ((e = ensure(c->pairs, sizeof(pp_pair), &grew)) || (e = ensure(c->counters, 64, &grew)))
     return alloc_fail(c, e, "pp_cuda_propagate_photons buffers");
+  if (grew) c->drop_graphs();
   if ((e = cudaMemcpyAsync(c->pairs.p, st_pair, sizeof(pp_pair), cudaMemcpyHostToDevice, s)))
     return c->cuda_fail(e, "copy source");
   pp::LaunchArgs a = base_args(c, opts);
@@ -739,7 +767,7 @@ pp_status pp_autotune(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp
   double photons = 0;
   for (int64_t i = 0; i < n_pairs; ++i) photons += (double)pairs[i].n_photons;
   if (photons <= 0) return c->fail(PP_ERR_ARG, "pp_autotune: no photons to time");
-  const int blocks[] = {128, 256, 512};
+  const int blocks[] = {128, 256};
   const int chunks[] = {1024, 4096, 16384};
   std::vector<pp_hit> hits(1 << 16);
   std::vector<double> stats((size_t)n_pairs * PP_STATS), hist((size_t)n_pairs * std::max(opts->hist_bins, 1));

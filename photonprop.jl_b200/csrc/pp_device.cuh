@@ -2,11 +2,13 @@
 //
 // One photon lives in registers: position, direction, path length, step
 // counter and two precomputed per-photon constants.  Its random numbers are
-// Philox4x32-10 blocks addressed by (photon index, block) under the pair's
-// seed, so nothing about the RNG is stored: block 0 holds the emission draws,
-// block k+1 the draws of step k, and the emission values (wavelength,
-// emission direction, emission time) are recomputed at a hit instead of
-// being kept live through the step loop.
+// Philox4x32-10 blocks under a fixed library key with the counter
+// (seed lo, seed hi, photon lo, photon hi | block << 8): the pair's 64-bit
+// seed, a photon index below 2^40 and a block below 2^24.  Nothing about the
+// RNG is stored: block 0 holds the emission draws, block k+1 the draws of
+// step k, and the emission values (wavelength, emission direction, emission
+// time) are recomputed at a hit instead of being kept live through the step
+// loop.  With the key fixed, the ten round keys are immediates.
 //
 // Transcendentals use the approximate MUFU instructions through inline PTX
 // (lg2/ex2/rcp/sqrt/sin/cos .approx); the rare hit path uses the accurate
@@ -94,9 +96,12 @@ __device__ __forceinline__ float u01(uint32_t w) {
   return __uint_as_float(0x3F800000u | (w >> 9)) - __uint_as_float(0x3F7FFFFFu);
 }
 
-__device__ __forceinline__ Draw4 draw_block(uint64_t photon, uint32_t block, uint32_t k0, uint32_t k1) {
-  uint32_t c[4] = {(uint32_t)photon, (uint32_t)(photon >> 32), block, 0u};
-  philox4x32_10(c, k0, k1);
+constexpr uint32_t kKey0 = 0x243F6A88u;  // fixed Philox key (hex digits of pi)
+constexpr uint32_t kKey1 = 0x85A308D3u;
+
+__device__ __forceinline__ Draw4 draw_block(uint32_t seed_lo, uint32_t seed_hi, uint64_t photon, uint32_t block) {
+  uint32_t c[4] = {seed_lo, seed_hi, (uint32_t)photon, (uint32_t)(photon >> 32) | (block << 8)};
+  philox4x32_10(c, kKey0, kKey1);
   return Draw4{u01(c[0]), u01(c[1]), u01(c[2]), u01(c[3])};
 }
 
@@ -202,55 +207,6 @@ __device__ __forceinline__ void rotate_to_axis(float ox, float oy, float oz, flo
   rz = z * f;
 }
 
-struct Emission {
-  float px, py, pz;
-  float dx, dy, dz;
-  float wl;
-  float t_emit;
-};
-
-// Emission of one photon from block 0 of its stream (src/photon_prop_cuda.jl:52-56,
-// 67-75, 308-316; the Cherenkov cone has no reference code: a point uniform
-// along the track, angle acos(1/n(wl)) about the track axis, time t0 + s/c).
-template <int MODE>
-__device__ __forceinline__ Emission emit_photon(const DevTables& T, const pp_pair& P, uint64_t photon,
-                                                uint32_t k0, uint32_t k1) {
-  const Draw4 d = draw_block(photon, 0u, k0, k1);
-  Emission e;
-  e.wl = draw_wavelength(T, d.u0);
-  // phi = 2 pi u2; evaluated as phi - pi in [-pi, pi) and negated.
-  const float ph = fmaf(kTwoPi, d.u2, -kPi);
-  const float sphi = -sin_a(ph), cphi = -cos_a(ph);
-  if (P.emitter == PP_EMITTER_ISOTROPIC) {
-    float st, ct;
-    if (MODE == kCompat) {  // theta = uniform(-1, 1) radians (reference quirk)
-      const float th = fmaf(2.f, d.u1, -1.f);
-      st = sin_a(th);
-      ct = cos_a(th);
-    } else {
-      ct = fmaf(2.f, d.u1, -1.f);
-      st = sqrt_a(fmaxf(0.f, fmaf(-ct, ct, 1.f)));
-    }
-    e.dx = cphi * st;
-    e.dy = sphi * st;
-    e.dz = ct;
-    e.px = P.pos[0];
-    e.py = P.pos[1];
-    e.pz = P.pos[2];
-    e.t_emit = P.t0;
-  } else {
-    const float ct = rcp(phase_index(T, rcp(e.wl)));
-    const float st = sqrt_a(fmaxf(0.f, fmaf(-ct, ct, 1.f)));
-    rotate_to_axis(P.dir[0], P.dir[1], P.dir[2], cphi * st, sphi * st, ct, e.dx, e.dy, e.dz);
-    const float s = d.u1 * P.track_len;
-    e.px = fmaf(s, P.dir[0], P.pos[0]);
-    e.py = fmaf(s, P.dir[1], P.pos[1]);
-    e.pz = fmaf(s, P.dir[2], P.pos[2]);
-    e.t_emit = fmaf(s, 1.f / kCVac, P.t0);
-  }
-  return e;
-}
-
 // Per-launch constants.
 struct RunParams {
   const pp_pair* __restrict__ pairs;
@@ -287,56 +243,121 @@ struct Photon {
 
 struct PairCtx {
   float tx, ty, tz, r2;
-  uint32_t k0, k1;
+  uint32_t seed_lo, seed_hi;
   int32_t index;
 };
 
-__device__ __forceinline__ PairCtx load_pair_ctx(const pp_pair& P, int index) {
+__device__ __forceinline__ PairCtx load_pair_ctx(const pp_pair* __restrict__ P, int index) {
+  const float4 t = __ldg(reinterpret_cast<const float4*>(P) + 2);  // target, radius
+  const uint2 sd = __ldg(reinterpret_cast<const uint2*>(P) + 7);   // seed
   PairCtx c;
-  c.tx = P.target[0];
-  c.ty = P.target[1];
-  c.tz = P.target[2];
-  c.r2 = P.radius * P.radius;
-  c.k0 = (uint32_t)P.seed;
-  c.k1 = (uint32_t)(P.seed >> 32);
+  c.tx = t.x;
+  c.ty = t.y;
+  c.tz = t.z;
+  c.r2 = t.w * t.w;
+  c.seed_lo = sd.x;
+  c.seed_hi = sd.y;
   c.index = index;
   return c;
 }
 
+// Where and how a photon is emitted, from block 0 of its stream
+// (src/photon_prop_cuda.jl:52-56, 67-75, 308-316).  The emission direction
+// is written as a polar angle about an axis, like a scattering: isotropic
+// emission is polar angle acos(2 u1 - 1) about e_z; the Cherenkov cone (no
+// reference code) is acos(1/n(wl)) about the track, from a point uniform
+// along the track at time t0 + s/c.  The reference-compatible isotropic
+// draw takes theta = 2 u1 - 1 radians (a reference quirk) and so carries its
+// own sin(theta).
+struct EmissionFrame {
+  float px, py, pz, t_emit, wl;
+  float ox, oy, oz;  // polar axis
+  float cpol, spol;  // spol valid only if has_spol
+  bool has_spol;
+};
+
 template <int MODE>
-__device__ __forceinline__ void start_photon(const DevTables& T, const pp_pair& P, const PairCtx& c,
-                                             const RunParams& R, uint64_t id, Photon& s) {
-  const Emission e = emit_photon<MODE>(T, P, id, c.k0, c.k1);
-  s.px = e.px;
-  s.py = e.py;
-  s.pz = e.pz;
-  s.dx = e.dx;
-  s.dy = e.dy;
-  s.dz = e.dz;
-  s.dist = 0.f;
-  s.k = 0;
-  s.id = id;
-  s.neg_ln2_len = -kLn2 * scattering_length(T, e.wl);
-  if (MODE == kPhysical) {
-    s.max_dist = (R.t_max - e.t_emit) * kCVac * rcp(group_index(T, rcp(e.wl)));
+__device__ __forceinline__ EmissionFrame emission_frame(const DevTables& T, const pp_pair* __restrict__ P,
+                                                        const Draw4& d) {
+  const float4 pt = __ldg(reinterpret_cast<const float4*>(P));      // pos, t0
+  const float4 dl = __ldg(reinterpret_cast<const float4*>(P) + 1);  // dir, track_len
+  const int emitter = __ldg(reinterpret_cast<const int*>(P) + 16);
+  EmissionFrame f;
+  f.wl = draw_wavelength(T, d.u0);
+  f.px = pt.x;
+  f.py = pt.y;
+  f.pz = pt.z;
+  f.t_emit = pt.w;
+  f.has_spol = false;
+  f.spol = 0.f;
+  if (emitter == PP_EMITTER_ISOTROPIC) {
+    f.ox = 0.f;
+    f.oy = 0.f;
+    f.oz = 1.f;
+    if (MODE == kCompat) {
+      const float th = fmaf(2.f, d.u1, -1.f);
+      f.cpol = cos_a(th);
+      f.spol = sin_a(th);
+      f.has_spol = true;
+    } else {
+      f.cpol = fmaf(2.f, d.u1, -1.f);
+    }
   } else {
-    s.max_dist = 3.0e38f;
+    f.ox = dl.x;
+    f.oy = dl.y;
+    f.oz = dl.z;
+    f.cpol = rcp(phase_index(T, rcp(f.wl)));
+    const float s = d.u1 * dl.w;
+    f.px = fmaf(s, f.ox, f.px);
+    f.py = fmaf(s, f.oy, f.py);
+    f.pz = fmaf(s, f.oz, f.pz);
+    f.t_emit = fmaf(s, 1.f / kCVac, f.t_emit);
   }
+  return f;
 }
 
-// One step of src/photon_prop_cuda.jl:320-376.  Returns false when the photon
-// ends; *hit is set when it ends on the sphere (position and path length
-// then point at the hit).
+// Unit vector at polar cos cpol (sin spol) and azimuth 2 pi u about the axis o
+// (update_direction, src/photon_prop_cuda.jl:223-241).  The azimuth is
+// evaluated as 2 pi u - pi in [-pi, pi) and the sine/cosine negated.
+__device__ __forceinline__ void polar_direction(float ox, float oy, float oz, float cpol, float spol, float u,
+                                                float& rx, float& ry, float& rz) {
+  const float ph = fmaf(kTwoPi, u, -kPi);
+  const float nx = -cos_a(ph) * spol, ny = -sin_a(ph) * spol;
+  rotate_to_axis(ox, oy, oz, nx, ny, cpol, rx, ry, rz);
+}
+
+__device__ __forceinline__ float sin_from_cos(float c) { return sqrt_a(fmaxf(0.f, fmaf(-c, c, 1.f))); }
+
+// Emission of photon s.id (block 0): position, direction and the
+// per-wavelength constants; afterwards s.k = 1.
 template <int MODE>
-__device__ __forceinline__ bool step_photon(const RunParams& R, const PairCtx& c, Photon& s, bool& hit) {
-  s.k += 1;
-  const Draw4 d = draw_block(s.id, (uint32_t)s.k, c.k0, c.k1);
+__device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
+                                           const PairCtx& c, Photon& s) {
+  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, 0u);
+  const EmissionFrame f = emission_frame<MODE>(T, P, d);
+  s.px = f.px;
+  s.py = f.py;
+  s.pz = f.pz;
+  s.dist = 0.f;
+  s.neg_ln2_len = -kLn2 * scattering_length(T, f.wl);
+  s.max_dist = (MODE == kPhysical) ? (R.t_max - f.t_emit) * kCVac * rcp(group_index(T, rcp(f.wl))) : 3.0e38f;
+  polar_direction(f.ox, f.oy, f.oz, f.cpol, f.has_spol ? f.spol : sin_from_cos(f.cpol), d.u2, s.dx, s.dy, s.dz);
+  s.k = 1;
+}
+
+// Step s.k - 1 (block s.k) of src/photon_prop_cuda.jl:320-376: step length,
+// ray-sphere test, move, Henyey-Greenstein turn.  Returns false when the
+// photon ends; *hit is set when it ends on the sphere (position and path
+// length then at the hit).
+template <int MODE>
+__device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c, Photon& s, bool& hit) {
+  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, (uint32_t)s.k);
+  bool alive = true;
   const float step = lg2(d.u0) * s.neg_ln2_len;
   const float ex = s.px - c.tx, ey = s.py - c.ty, ez = s.pz - c.tz;
   const float a = fmaf(s.dz, ez, fmaf(s.dy, ey, s.dx * ex));
   const float pp = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
   const float b = fmaf(a, a, c.r2 - pp);
-  bool alive = true;
   bool move = true;
   if (b >= 0.f) {
     const float dd = -a - sqrt_a(b);
@@ -354,48 +375,63 @@ __device__ __forceinline__ bool step_photon(const RunParams& R, const PairCtx& c
       move = false;  // the line meets the sphere outside this step: no move (reference)
     }
   }
-  if (move) {
-    if (MODE == kPhysical && s.dist + step > s.max_dist) {
-      alive = false;
-    } else {
-      s.px = fmaf(step, s.dx, s.px);
-      s.py = fmaf(step, s.dy, s.py);
-      s.pz = fmaf(step, s.dz, s.pz);
-      s.dist += step;
-      const float ct = hg_costheta(R.hg, d.u1);
-      const float st = sqrt_a(fmaxf(0.f, fmaf(-ct, ct, 1.f)));
-      const float ph = fmaf(kTwoPi, d.u2, -kPi);
-      const float nx = -cos_a(ph) * st, ny = -sin_a(ph) * st;
-      rotate_to_axis(s.dx, s.dy, s.dz, nx, ny, ct, s.dx, s.dy, s.dz);
-    }
+  if (move && MODE == kPhysical && s.dist + step > s.max_dist) {
+    move = false;
+    alive = false;
   }
-  if (s.k >= R.max_steps) alive = false;
+  if (move) {
+    s.px = fmaf(step, s.dx, s.px);
+    s.py = fmaf(step, s.dy, s.py);
+    s.pz = fmaf(step, s.dz, s.pz);
+    s.dist += step;
+  }
+  const float cpol = hg_costheta(R.hg, d.u1);
+  float rx, ry, rz;
+  polar_direction(s.dx, s.dy, s.dz, cpol, sin_from_cos(cpol), d.u2, rx, ry, rz);
+  if (move) {
+    s.dx = rx;
+    s.dy = ry;
+    s.dz = rz;
+  }
+  s.k += 1;
+  if (s.k > R.max_steps) alive = false;  // s.k - 1 steps taken
   return alive;
 }
 
-// Everything a hit record needs (src/photon_prop_cuda.jl:622,634-641).
+// Emission (s.k == 0) or step event of one photon.
+template <int MODE>
+__device__ __forceinline__ bool photon_event(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
+                                             const PairCtx& c, Photon& s, bool& hit) {
+  if (s.k == 0) {
+    emit_event<MODE>(T, R, P, c, s);
+    return true;
+  }
+  return step_event<MODE>(R, c, s, hit);
+}
+
+// Everything a hit record needs (src/photon_prop_cuda.jl:622,634-641); the
+// emission is replayed from block 0 with the same arithmetic as its event.
 struct HitValues {
   float time, weight, wl;
   float d0x, d0y, d0z;
 };
 
 template <int MODE>
-__device__ __forceinline__ HitValues hit_values(const DevTables& T, const RunParams& R, const pp_pair& P,
+__device__ __forceinline__ HitValues hit_values(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                                 const PairCtx& c, const Photon& s) {
-  const Emission e = emit_photon<MODE>(T, P, s.id, c.k0, c.k1);
+  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, 0u);
+  const EmissionFrame f = emission_frame<MODE>(T, P, d);
   HitValues h;
-  h.wl = e.wl;
-  h.d0x = e.dx;
-  h.d0y = e.dy;
-  h.d0z = e.dz;
-  const float x = 1.f / e.wl;
+  h.wl = f.wl;
+  polar_direction(f.ox, f.oy, f.oz, f.cpol, f.has_spol ? f.spol : sin_from_cos(f.cpol), d.u2, h.d0x, h.d0y, h.d0z);
+  const float x = 1.f / f.wl;
   if (MODE == kCompat) {
     h.time = s.dist * phase_index(T, x) / kCVac;  // phase velocity (reference)
   } else {
-    h.time = e.t_emit + s.dist * group_index(T, x) / kCVac;
+    h.time = f.t_emit + s.dist * group_index(T, x) / kCVac;
   }
-  float w = expf(-s.dist / interp_sorted(e.wl, T.abs_wl, T.abs_len, T.n_abs));
-  if ((R.flags & PP_OPT_PMT_WEIGHT) && T.n_pmt > 0) w *= interp_sorted(e.wl, T.pmt_wl, T.pmt_acc, T.n_pmt);
+  float w = expf(-s.dist / interp_sorted(f.wl, T.abs_wl, T.abs_len, T.n_abs));
+  if ((R.flags & PP_OPT_PMT_WEIGHT) && T.n_pmt > 0) w *= interp_sorted(f.wl, T.pmt_wl, T.pmt_acc, T.n_pmt);
   h.weight = w;
   return h;
 }

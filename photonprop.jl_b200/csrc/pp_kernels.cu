@@ -23,87 +23,148 @@ namespace ppd {
 
 // ---------------------------------------------------------------------------
 // Batched persistent kernel.
-template <int MODE>
-__global__ void __launch_bounds__(512) batched_kernel(const RunParams R) {
+//
+// Each warp owns a ring of kStage staged emissions in shared memory.  When
+// its dead lanes outnumber the staged photons, all 32 lanes take the next
+// photon indices from the warp's chunk (grabbing chunks from the device work
+// queue) and compute 32 emissions together, converged; dead lanes then pick
+// staged photons up with three 16-byte loads.  The step loop that follows
+// is the same straight-line code for every lane.
+constexpr int kStage = 64;  // >= 2 * 32 - 1 staged emissions per warp (power of two)
+
+struct __align__(16) Staged {
+  float px, py, pz, dx, dy, dz, neg_ln2_len, max_dist;
+  uint32_t id_lo, id_hi;
+  int32_t pair;
+  uint32_t pad;
+};
+
+template <int MODE, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32) batched_kernel(const RunParams R) {
   __shared__ __align__(16) DevTables T;
+  __shared__ Staged stage[WARPS][kStage];
   stage_tables(T, R.tables);
   __syncthreads();
 
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
+  Staged* ring = stage[threadIdx.x >> 5];
   const unsigned long long total_chunks = R.chunk_offsets[R.n_pairs];
 
-  // warp-uniform work state
-  unsigned long long c_next = 0, c_end = 0;
+  // warp-uniform state: the current chunk and the ring
+  unsigned long long c_base = 0;  // first photon index of the chunk
+  unsigned c_next = 0, c_len = 0;
   int c_pair = 0;
-  bool warp_done = false;
+  bool queue_done = false;
+  unsigned r_head = 0, r_count = 0;
 
   // lane state
   bool alive = false;
-  bool fresh = false;
-  int pair = 0;
   Photon s;
   s.id = 0;
+  s.k = 1;
+  s.px = s.py = s.pz = s.dx = s.dy = s.dist = s.neg_ln2_len = s.max_dist = 0.f;
+  s.dz = 1.f;
   PairCtx c;
+  c.tx = c.ty = c.tz = c.r2 = 0.f;
+  c.seed_lo = c.seed_hi = 0u;
   c.index = 0;
   unsigned steps = 0;
 
   for (;;) {
-    unsigned need = __ballot_sync(kFull, !alive);
-    fresh = false;
-    while (need != 0u && !warp_done) {
-      if (c_next >= c_end) {
-        unsigned long long cid = 0, start = 0, end = 0;
-        int p = 0;
-        if (lane == 0) {
-          cid = atomicAdd(R.queue, 1ull);
-          if (cid < total_chunks) {
-            int lo = 0, hi = (int)R.n_pairs - 1;  // last pair with offset <= cid
-            while (lo < hi) {
-              const int mid = (lo + hi + 1) >> 1;
-              if (R.chunk_offsets[mid] <= cid) lo = mid; else hi = mid - 1;
+    const unsigned need = __ballot_sync(kFull, !alive);
+    const unsigned n_need = __popc(need);
+    if (r_count < n_need && !queue_done) {
+      // give every lane the next photon index of the queue
+      bool have = false;
+      unsigned long long pid = 0;
+      int ppair = 0;
+      unsigned filled = 0;
+      while (filled < 32u) {
+        if (c_next >= c_len) {
+          unsigned long long cid = 0, start = 0, end = 0;
+          int p = 0;
+          if (lane == 0) {
+            cid = atomicAdd(R.queue, 1ull);
+            if (cid < total_chunks) {
+              int lo = 0, hi = (int)R.n_pairs - 1;  // last pair whose first chunk <= cid
+              while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (R.chunk_offsets[mid] <= cid) lo = mid; else hi = mid - 1;
+              }
+              p = lo;
+              start = (cid - R.chunk_offsets[p]) * (unsigned long long)R.chunk;
+              end = min(start + (unsigned long long)R.chunk, (unsigned long long)R.pairs[p].n_photons);
             }
-            p = lo;
-            start = (cid - R.chunk_offsets[p]) * (unsigned long long)R.chunk;
-            const unsigned long long n = (unsigned long long)R.pairs[p].n_photons;
-            end = min(start + (unsigned long long)R.chunk, n);
           }
+          cid = __shfl_sync(kFull, cid, 0);
+          if (cid >= total_chunks) {
+            queue_done = true;
+            break;
+          }
+          c_pair = __shfl_sync(kFull, p, 0);
+          c_base = __shfl_sync(kFull, start, 0);
+          c_len = (unsigned)(__shfl_sync(kFull, end, 0) - c_base);
+          c_next = 0;
         }
-        cid = __shfl_sync(kFull, cid, 0);
-        if (cid >= total_chunks) {
-          warp_done = true;
-          break;
+        const unsigned take = min(32u - filled, c_len - c_next);
+        if (lane >= filled && lane < filled + take) {
+          have = true;
+          pid = c_base + (c_next + (lane - filled));
+          ppair = c_pair;
         }
-        c_pair = __shfl_sync(kFull, p, 0);
-        c_next = __shfl_sync(kFull, start, 0);
-        c_end = __shfl_sync(kFull, end, 0);
+        c_next += take;
+        filled += take;
       }
-      const unsigned avail = (unsigned)min(c_end - c_next, 32ull);
+      if (have) {
+        const pp_pair* P = R.pairs + ppair;
+        const PairCtx pc = load_pair_ctx(P, ppair);
+        Photon e;
+        e.id = pid;
+        emit_event<MODE>(T, R, P, pc, e);
+        float4* dst = reinterpret_cast<float4*>(ring + ((r_head + r_count + lane) & (kStage - 1)));
+        dst[0] = make_float4(e.px, e.py, e.pz, e.dx);
+        dst[1] = make_float4(e.dy, e.dz, e.neg_ln2_len, e.max_dist);
+        dst[2] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)),
+                             __int_as_float(ppair), 0.f);
+      }
+      r_count += filled;
+      __syncwarp();
+    }
+    if (!alive) {
       const unsigned rank = __popc(need & lt_mask);
-      if (!alive && rank < avail) {
-        pair = c_pair;
-        s.id = c_next + rank;
+      if (rank < r_count) {
+        const float4* src = reinterpret_cast<const float4*>(ring + ((r_head + rank) & (kStage - 1)));
+        const float4 a = src[0], b = src[1], d = src[2];
+        s.px = a.x;
+        s.py = a.y;
+        s.pz = a.z;
+        s.dx = a.w;
+        s.dy = b.x;
+        s.dz = b.y;
+        s.neg_ln2_len = b.z;
+        s.max_dist = b.w;
+        s.dist = 0.f;
+        s.k = 1;
+        s.id = ((unsigned long long)__float_as_uint(d.y) << 32) | __float_as_uint(d.x);
+        const int pr = __float_as_int(d.z);
+        c = load_pair_ctx(R.pairs + pr, pr);
         alive = true;
-        fresh = true;
       }
-      c_next += min((unsigned)__popc(need), avail);
-      need = __ballot_sync(kFull, !alive);
     }
-    if (fresh) {
-      const pp_pair P = R.pairs[pair];
-      c = load_pair_ctx(P, pair);
-      start_photon<MODE>(T, P, c, R, s.id, s);
-    }
+    const unsigned took = min(n_need, r_count);
+    r_head += took;
+    r_count -= took;
+    __syncwarp();
     if (__ballot_sync(kFull, alive) == 0u) break;
     bool hit = false;
     if (alive) {
       ++steps;
-      alive = step_photon<MODE>(R, c, s, hit);
+      alive = step_event<MODE>(R, c, s, hit);
     }
     if (__any_sync(kFull, hit)) {
       if (hit) {
-        const pp_pair P = R.pairs[c.index];
-        const HitValues h = hit_values<MODE>(T, R, P, c, s);
+        const HitValues h = hit_values<MODE>(T, R, R.pairs + c.index, c, s);
         record_hit(R, c, s, h, c.index);
       }
     }
@@ -123,22 +184,24 @@ __global__ void __launch_bounds__(512) plain_kernel(const RunParams R, const pp_
   __shared__ __align__(16) DevTables T;
   stage_tables(T, R.tables);
   __syncthreads();
-  const pp_pair P = *pair_ptr;
-  const PairCtx c = load_pair_ctx(P, pair_index);
-  const unsigned long long n = (unsigned long long)P.n_photons;
+  const PairCtx c = load_pair_ctx(pair_ptr, pair_index);
+  const unsigned long long n = (unsigned long long)pair_ptr->n_photons;
   const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
   unsigned steps = 0;
   for (unsigned long long id = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; id < n;
        id += stride) {
     Photon s;
-    start_photon<MODE>(T, P, c, R, id, s);
+    s.id = id;
+    s.k = 0;
+    s.dx = s.dy = 0.f;
+    s.dz = 1.f;
     bool alive = true;
     while (alive) {
       bool hit = false;
-      ++steps;
-      alive = step_photon<MODE>(R, c, s, hit);
+      steps += (s.k > 0);
+      alive = photon_event<MODE>(T, R, pair_ptr, c, s, hit);
       if (hit) {
-        const HitValues h = hit_values<MODE>(T, R, P, c, s);
+        const HitValues h = hit_values<MODE>(T, R, pair_ptr, c, s);
         record_hit(R, c, s, h, 0);
       }
     }
@@ -165,8 +228,7 @@ __global__ void __launch_bounds__(1024) stacks_kernel(const RunParams R, const p
   const int ix_offset = (int)blockIdx.x * stack_len + 1;  // 1-based, as in the reference
   if (threadIdx.x == 0) cursor = ix_offset;
   __syncthreads();
-  const pp_pair P = *pair_ptr;
-  const PairCtx c = load_pair_ctx(P, 0);
+  const PairCtx c = load_pair_ctx(pair_ptr, 0);
   const int safe_margin = max(0, (int)blockDim.x - 32);
   const unsigned long long G = (unsigned long long)gridDim.x * blockDim.x;
   const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -175,24 +237,27 @@ __global__ void __launch_bounds__(1024) stacks_kernel(const RunParams R, const p
   for (long long i = 0; i < per_thread; ++i) {
     if (*(volatile int*)&cursor > ix_offset + stack_len - safe_margin) break;
     Photon s;
-    start_photon<MODE>(T, P, c, R, g + (unsigned long long)i * G, s);
+    s.id = g + (unsigned long long)i * G;
+    s.k = 0;
+    s.dx = s.dy = 0.f;
+    s.dz = 1.f;
     bool alive = true;
     while (alive) {
       bool hit = false;
-      ++steps;
-      alive = step_photon<MODE>(R, c, s, hit);
+      steps += (s.k > 0);
+      alive = photon_event<MODE>(T, R, pair_ptr, c, s, hit);
       if (hit) {
-        const Emission e = emit_photon<MODE>(T, P, s.id, c.k0, c.k1);
+        const HitValues h = hit_values<MODE>(T, R, pair_ptr, c, s);
         const int idx = atomicAdd(&cursor, 1);  // 1-based slot
         if (idx < ix_offset + stack_len) {
           const int j = idx - 1;
           out_pos[3 * j + 0] = s.px;
           out_pos[3 * j + 1] = s.py;
           out_pos[3 * j + 2] = s.pz;
-          out_dir[3 * j + 0] = e.dx;
-          out_dir[3 * j + 1] = e.dy;
-          out_dir[3 * j + 2] = e.dz;
-          out_wl[j] = e.wl;
+          out_dir[3 * j + 0] = h.d0x;
+          out_dir[3 * j + 1] = h.d0y;
+          out_dir[3 * j + 2] = h.d0z;
+          out_wl[j] = h.wl;
           out_dist[j] = s.dist;
           atomicMax(out_sp + blockIdx.x, idx);
         } else {
@@ -363,18 +428,15 @@ __global__ void peak_mufu_kernel(float* out, int iters) {
   if (s == 1.2345f) out[0] = s;
 }
 
-__global__ void peak_int_kernel(unsigned* out, int iters) {
-  unsigned x[8];
-#pragma unroll
-  for (int j = 0; j < 8; ++j) x[j] = threadIdx.x * 2654435761u + j;
+__global__ void peak_philox_kernel(unsigned* out, int iters) {
+  // independent Philox4x32-10 blocks per thread: the integer work of one photon step
+  uint32_t acc = 0;
   for (int i = 0; i < iters; ++i) {
-#pragma unroll
-    for (int j = 0; j < 8; ++j) x[j] = x[j] * 0x9E3779B9u + 0x7F4A7C15u;  // IMAD
+    uint32_t c[4] = {threadIdx.x, blockIdx.x, (uint32_t)i, 0u};
+    philox4x32_10(c, 0x12345678u, 0x9abcdef0u);
+    acc ^= c[0] ^ c[1] ^ c[2] ^ c[3];
   }
-  unsigned s = 0;
-#pragma unroll
-  for (int j = 0; j < 8; ++j) s ^= x[j];
-  if (s == 12345u) out[0] = s;
+  if (acc == 12345u) out[0] = acc;
 }
 
 }  // namespace ppd
@@ -465,10 +527,17 @@ cudaError_t launch_reset_counters(unsigned long long* counters, cudaStream_t s) 
 
 cudaError_t launch_batched(const LaunchArgs& a, int grid, int block, cudaStream_t s) {
   const ppd::RunParams R = to_params(a);
-  if (a.opts.mode == PP_MODE_COMPAT)
-    ppd::batched_kernel<ppd::kCompat><<<grid, block, 0, s>>>(R);
-  else
-    ppd::batched_kernel<ppd::kPhysical><<<grid, block, 0, s>>>(R);
+  if (block == 128) {
+    if (a.opts.mode == PP_MODE_COMPAT)
+      ppd::batched_kernel<ppd::kCompat, 4><<<grid, 128, 0, s>>>(R);
+    else
+      ppd::batched_kernel<ppd::kPhysical, 4><<<grid, 128, 0, s>>>(R);
+  } else {
+    if (a.opts.mode == PP_MODE_COMPAT)
+      ppd::batched_kernel<ppd::kCompat, 8><<<grid, 256, 0, s>>>(R);
+    else
+      ppd::batched_kernel<ppd::kPhysical, 8><<<grid, 256, 0, s>>>(R);
+  }
   count_launches(1);
   return cudaGetLastError();
 }
@@ -519,10 +588,17 @@ cudaError_t launch_eval(int op, const double* in, double* out, int64_t n, const 
 
 int batched_max_blocks_per_sm(int mode, int block) {
   int nb = 0;
-  if (mode == PP_MODE_COMPAT)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kCompat>, block, 0);
-  else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical>, block, 0);
+  if (block == 128) {
+    if (mode == PP_MODE_COMPAT)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kCompat, 4>, 128, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical, 4>, 128, 0);
+  } else {
+    if (mode == PP_MODE_COMPAT)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kCompat, 8>, 256, 0);
+    else
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical, 8>, 256, 0);
+  }
   return nb;
 }
 
@@ -548,9 +624,9 @@ cudaError_t run_peaks(int sm_count, double* fp32, double* mufu, double* iops) {
   // warm-up
   ppd::peak_fma_kernel<<<grid, block>>>(dout, 1000, 0.999f, 0.001f);
   ppd::peak_mufu_kernel<<<grid, block>>>(dout, 100);
-  ppd::peak_int_kernel<<<grid, block>>>(reinterpret_cast<unsigned*>(dout), 100);
+  ppd::peak_philox_kernel<<<grid, block>>>(reinterpret_cast<unsigned*>(dout), 100);
   count_launches(3);
-  const int it_f = 20000, it_m = 4000, it_i = 10000;
+  const int it_f = 20000, it_m = 40000, it_i = 4000;
   cudaEventRecord(a);
   ppd::peak_fma_kernel<<<grid, block>>>(dout, it_f, 0.999f, 0.001f);
   cudaEventRecord(b);
@@ -564,11 +640,11 @@ cudaError_t run_peaks(int sm_count, double* fp32, double* mufu, double* iops) {
   cudaEventElapsedTime(&ms, a, b);
   *mufu = threads * it_m * 8.0 / (ms * 1e-3);
   cudaEventRecord(a);
-  ppd::peak_int_kernel<<<grid, block>>>(reinterpret_cast<unsigned*>(dout), it_i);
+  ppd::peak_philox_kernel<<<grid, block>>>(reinterpret_cast<unsigned*>(dout), it_i);
   cudaEventRecord(b);
   cudaEventSynchronize(b);
   cudaEventElapsedTime(&ms, a, b);
-  *iops = threads * it_i * 8.0 / (ms * 1e-3);
+  *iops = threads * it_i / (ms * 1e-3);  // Philox blocks per second
   count_launches(3);
   e = cudaGetLastError();
   cudaEventDestroy(a);

@@ -28,9 +28,10 @@ def launch_count() -> int:
 
 
 def measure_peaks(device=0):
-    """FP32 FMA, MUFU and INT multiply-add issue peaks of the device (ops/s)."""
+    """FP32 FMA and MUFU issue peaks (ops/s) and the Philox4x32-10 block rate
+    (blocks/s) of the device."""
     import ctypes
     L = _lib.load()
     f, m, i = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
     _lib.check(L.pp_measure_peaks(device, ctypes.byref(f), ctypes.byref(m), ctypes.byref(i)))
-    return {"fp32_ops": f.value, "mufu_ops": m.value, "int_ops": i.value}
+    return {"fp32_ops": f.value, "mufu_ops": m.value, "philox_blocks": i.value}

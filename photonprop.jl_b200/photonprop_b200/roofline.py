@@ -7,23 +7,23 @@ per photon step   6 MUFU  (lg2 step length, rcp HG, sqrt sin(theta), sin, cos,
                  51 FP32  (FFMA/FMUL/FADD: uniforms 3, step 1, ray-sphere 11,
                            move 4, HG 4, sin(theta) 1, azimuth 3, rotation with
                            Newton renormalisation 24)
-                 60 INT   (one Philox4x32-10 block: 10 rounds of 2 IMAD.WIDE,
-                           2 LOP3, 2 IADD)
+                  1 Philox4x32-10 block (10 rounds of 2 IMAD.WIDE, 2 LOP3, 2 IADD)
 per photon start  isotropic: 10 MUFU, 25 FP32; Cherenkov cone: 14 MUFU, 57 FP32;
                   plus one Philox block.
+A photon that hits the sphere also re-draws its emission block (rare).
 """
 
 MUFU_PER_STEP = 6
 FP32_PER_STEP = 51
-INT_PER_STEP = 60
+PHILOX_PER_STEP = 1
 MUFU_PER_PHOTON = {0: 10, 1: 14}   # by emitter type
 FP32_PER_PHOTON = {0: 25, 1: 57}
-INT_PER_PHOTON = 60
+PHILOX_PER_PHOTON = 1
 
 
 def op_counts(steps, photons_iso, photons_cone):
-    """(mufu, fp32, int) operations for a run."""
+    """(mufu, fp32, philox blocks) for a run."""
     mufu = steps * MUFU_PER_STEP + photons_iso * MUFU_PER_PHOTON[0] + photons_cone * MUFU_PER_PHOTON[1]
     fp32 = steps * FP32_PER_STEP + photons_iso * FP32_PER_PHOTON[0] + photons_cone * FP32_PER_PHOTON[1]
-    iops = (steps + photons_iso + photons_cone) * INT_PER_STEP
-    return mufu, fp32, iops
+    blocks = steps * PHILOX_PER_STEP + (photons_iso + photons_cone) * PHILOX_PER_PHOTON
+    return mufu, fp32, blocks

@@ -4,7 +4,7 @@ Tolerances (FP32 photon state against the FP64 oracle replaying the same
 Philox numbers):
   device helpers      philox / uniform bit-exact; HG, rotation, medium rel/abs 2e-5
   matched photons     |d pos| <= 2e-3 m + 2e-5 * path, |d t| <= 1e-2 ns + 1e-5 * t,
-                      |d w| / w <= 1e-3, |d lambda| / lambda <= 1e-5
+                      |d w| <= 1e-3 w + 1e-8, |d lambda| / lambda <= 1e-5
   branch flips        photons detected on one side only <= 1 % of hits (+3)
 """
 import numpy as np
@@ -29,7 +29,8 @@ def _check_matched(g, o, n_gpu_only, n_orc_only, label):
     path = o["dist"]
     assert np.all(err["pos"] <= 2e-3 + 2e-5 * path), (label, s["pos"])
     assert np.all(err["time"] <= 1e-2 + 1e-5 * o["time"]), (label, s["time"])
-    assert np.all(err["weight"] <= 1e-3), (label, s["weight"])
+    # relative 1e-3, plus an absolute floor where the PMT acceptance tends to zero
+    assert np.all(np.abs(g["weight"] - o["weight"]) <= 1e-3 * o["weight"] + 1e-8), (label, s["weight"])
     assert np.all(err["wavelength"] <= 1e-5), (label, s["wavelength"])
     return s
 
@@ -79,7 +80,9 @@ def test_device_rotate_to_axis(propagator):
     n /= np.linalg.norm(n, axis=1, keepdims=True)
     o32, n32 = o.astype(np.float32).astype(np.float64), n.astype(np.float32).astype(np.float64)
     out = propagator.device_eval(3, np.concatenate([o32, n32], 1))
-    ref = np.array([O.rotate_to_axis(a, b) for a, b in zip(o32, n32)])
+    # reference on exactly normalised inputs: its sin(theta) = sqrt(1 - o_z^2) is
+    # ill-conditioned near the poles for vectors that are unit only to FP32 rounding
+    ref = np.array([O.rotate_to_axis(a / np.linalg.norm(a), b / np.linalg.norm(b)) for a, b in zip(o32, n32)])
     err = np.linalg.norm(out - ref, axis=1)
     far = np.abs(o32[:, 2] + 1) > 1e-3  # away from the south pole the rotation is well conditioned
     assert err[far].max() < 2e-6
