@@ -208,6 +208,30 @@ PP_API pp_status pp_propagate_device(pp_ctx* ctx, const pp_pair* d_pairs, int64_
                               uint64_t* d_counters, double* d_stats, double* d_hist,
                               void* stream);
 
+/* Allocation-free form of pp_propagate_device.  It has no counterpart in the
+ * reference.  It exists for callers that own all device memory through their
+ * own pool and cannot let a library call cudaMalloc behind their back: Julia's
+ * CUDA.jl allocator or PyTorch's caching allocator may hold the free memory,
+ * so a library cudaMalloc can fail, and cudaMalloc/cudaFree can synchronise
+ * the device in the middle of the caller's stream work.  The work-queue
+ * scratch (chunk offsets and queue cursor) lives in one static device array
+ * of (PP_NOALLOC_MAX_PAIRS + 33) x 8 bytes (about 512 KiB) that every GPU
+ * which loads the library holds until the process exits.  The call allocates
+ * nothing, launches directly (no graph) and otherwise behaves like
+ * pp_propagate_device.  Limits and rules:
+ *  - n_pairs above PP_NOALLOC_MAX_PAIRS is rejected with PP_ERR_ARG;
+ *  - the first call on a device looks up the array's device address (once per
+ *    device, with that device current); make that first call before any stream
+ *    capture;
+ *  - all calls share the array and it keeps the last call's contents (each
+ *    call resets what must start at zero), so calls that overlap on the GPU
+ *    race: issue them on one stream or otherwise serialise them. */
+#define PP_NOALLOC_MAX_PAIRS 65536
+PP_API pp_status pp_propagate_device_noalloc(pp_ctx* ctx, const pp_pair* d_pairs, int64_t n_pairs,
+                                             const pp_run_opts* opts, pp_hit* d_hits, int64_t hit_capacity,
+                                             uint64_t* d_counters, double* d_stats, double* d_hist,
+                                             void* stream);
+
 /* Device-buffer form of the plain kernel for one pair (no graph). */
 PP_API pp_status pp_propagate_plain_device(pp_ctx* ctx, const pp_pair* d_pair, const pp_pair* h_pair,
                                     int64_t pair_index, const pp_run_opts* opts, pp_hit* d_hits,

@@ -817,3 +817,78 @@ pp_status pp_autotune(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free batched propagation (pp_propagate_device_noalloc).
+//
+// The work-queue scratch is this file-scope device array: word 0 is the queue
+// cursor, words 32.. the chunk offsets (n_pairs + 1 of them).  In host code
+// the name g_noalloc_scratch is only a host-side stand-in for the symbol, not
+// a device address: a kernel given it would fault or, where the GPU can reach
+// host memory, silently use the wrong memory.  The device address is looked
+// up once per device with cudaGetSymbolAddress (with that device current) and
+// cached.
+namespace {
+constexpr int kNoallocQueueWords = 32;
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoallocQueueWords + PP_NOALLOC_MAX_PAIRS + 1];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+unsigned long long* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array on the current device (set-up on first use).
+cudaError_t noalloc_scratch(int device, unsigned long long** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
+  if (!g_noalloc_ptr[device]) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    g_noalloc_ptr[device] = static_cast<unsigned long long*>(p);
+  }
+  *out = g_noalloc_ptr[device];
+  return cudaSuccess;
+}
+}  // namespace
+
+extern "C" pp_status pp_propagate_device_noalloc(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs,
+                                                 const pp_run_opts* opts, pp_hit* d_hits, int64_t cap,
+                                                 uint64_t* d_counters, double* d_stats, double* d_hist,
+                                                 void* stream) {
+  if (!c) return PP_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  pp_status st = validate_opts(c, opts);
+  if (st) return st;
+  if (n_pairs > PP_NOALLOC_MAX_PAIRS)
+    return c->fail(PP_ERR_ARG, "pp_propagate_device_noalloc: n_pairs exceeds PP_NOALLOC_MAX_PAIRS (65536); "
+                               "split the batch or use pp_propagate_device");
+  if (n_pairs < 0 || (n_pairs > 0 && !d_pairs) || !d_counters || !d_stats || (opts->hist_bins > 0 && !d_hist) ||
+      cap < 0 || (cap > 0 && !d_hits))
+    return c->fail(PP_ERR_ARG, "pp_propagate_device_noalloc: bad buffer arguments");
+  if (!aligned(d_pairs, 16) || !aligned(d_hits, 16) || !aligned(d_counters, 8) || !aligned(d_stats, 8) ||
+      !aligned(d_hist, 8))
+    return c->fail(PP_ERR_ARG,
+                   "pp_propagate_device_noalloc: pairs/hits need 16-byte, counters/stats/hist 8-byte alignment");
+  DeviceGuard guard(c->device);
+  unsigned long long* scratch = nullptr;
+  cudaError_t e = noalloc_scratch(c->device, &scratch);
+  if (e) return c->cuda_fail(e, "pp_propagate_device_noalloc: cudaGetSymbolAddress");
+  int grid, block;
+  uint32_t chunk;
+  resolve_launch(c, *opts, grid, block, chunk);
+  pp::LaunchArgs a = base_args(c, opts);
+  a.pairs = d_pairs;
+  a.n_pairs = n_pairs;
+  a.queue = scratch;
+  a.chunk_offsets = scratch + kNoallocQueueWords;
+  a.chunk = chunk;
+  a.hits = d_hits;
+  a.hit_cap = (unsigned long long)cap;
+  a.counters = reinterpret_cast<unsigned long long*>(d_counters);
+  a.stats = d_stats;
+  a.hist = opts->hist_bins > 0 ? d_hist : nullptr;
+  // the scan kernel rewrites every offset and zeroes the cursor and counters
+  if ((e = enqueue_batched(c, a, grid, block, static_cast<cudaStream_t>(stream))))
+    return c->cuda_fail(e, "pp_propagate_device_noalloc");
+  return PP_OK;
+}

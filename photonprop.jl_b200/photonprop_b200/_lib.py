@@ -22,6 +22,7 @@ EMITTER_ISOTROPIC, EMITTER_CHERENKOV_CONE = 0, 1
 SPECTRUM_CHERENKOV, SPECTRUM_MONOCHROMATIC = 0, 1
 OPT_PMT_WEIGHT, OPT_NORMALIZE, OPT_NO_HITS = 1, 2, 4
 MAX_KNOTS, MAX_ABS, MAX_PMT, N_STATS = 64, 32, 256, 8
+NOALLOC_MAX_PAIRS = 65536
 
 PAIR_DTYPE = np.dtype([
     ("pos", "<f4", 3), ("t0", "<f4"), ("dir", "<f4", 3), ("track_len", "<f4"),
@@ -99,6 +100,8 @@ _SIGS = [
                                           ctypes.POINTER(_I64), _VP, _VP]),
     ("pp_propagate_device", ctypes.c_int, [_VP, _VP, _I64, ctypes.POINTER(RunOpts), _VP, _I64,
                                            _VP, _VP, _VP, _VP]),
+    ("pp_propagate_device_noalloc", ctypes.c_int, [_VP, _VP, _I64, ctypes.POINTER(RunOpts), _VP, _I64,
+                                                   _VP, _VP, _VP, _VP]),
     ("pp_propagate_plain_device", ctypes.c_int, [_VP, _VP, _VP, _I64, ctypes.POINTER(RunOpts), _VP,
                                                  _I64, _VP, _VP, _VP, _VP]),
     ("pp_cuda_propagate_photons", ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _I32, _I32, _I32,

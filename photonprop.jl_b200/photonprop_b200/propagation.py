@@ -200,6 +200,20 @@ class Propagator:
             _lib.ptr(d_counters), _lib.ptr(d_stats), _lib.ptr(d_hist) if o.hist_bins > 0 else None,
             s), self._h)
 
+    def propagate_device_noalloc(self, d_pairs, n_pairs, opts: RunOptions, d_hits, hit_capacity, d_counters,
+                                 d_stats, d_hist, stream=None):
+        """pp_propagate_device_noalloc: like propagate_device, for callers whose
+        device memory is all owned by their own pool; the library allocates
+        nothing (its work-queue scratch is a fixed static device array, at most
+        NOALLOC_MAX_PAIRS pairs per call).  Make the first call on a device
+        before any stream capture, and do not overlap calls on the GPU."""
+        o = opts.to_c()
+        s = getattr(stream, "cuda_stream", stream)
+        _lib.check(self._L.pp_propagate_device_noalloc(
+            self._h, _lib.ptr(d_pairs), n_pairs, ctypes.byref(o), _lib.ptr(d_hits), hit_capacity,
+            _lib.ptr(d_counters), _lib.ptr(d_stats), _lib.ptr(d_hist) if o.hist_bins > 0 else None,
+            s), self._h)
+
     def propagate_plain_device(self, d_pair, h_pair, pair_index, opts: RunOptions, d_hits, hit_capacity,
                                d_counters, d_stats, d_hist, stream=None):
         o = opts.to_c()
