@@ -361,7 +361,11 @@ def run_ours(args):
         "latency_ms": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                        "what": "device time of one 4096-pair batch solve"},
         "roofline": {"bound": "mufu", "achieved": a_mufu / 1e9, "peak": peaks["mufu_ops"] / 1e9,
-                     "unit": "Gop/s", "frac": f_mufu, "traffic": None,
+                     "unit": "Gop/s", "frac": f_mufu,
+                     "traffic": roofline.NCU_DRAM_BYTES_PER_PHOTON * photons_local[0],
+                     "traffic_note": "DRAM bytes per launch: ncu capture of a 2.5e8-photon launch scaled by photons",
+                     "issue_active_ncu": roofline.NCU_ISSUE_ACTIVE,
+                     "note": "issue-bound: ncu shows 79% of issue slots busy (ALU pipe 54%, FMA 34%, XU 27%)",
                      "peak_source": "measured live: ex2.approx dependent chains over every SM (pp_measure_peaks)",
                      "fp32": {"achieved": a_fp32 / 1e9, "peak": peaks["fp32_ops"] / 1e9, "frac": f_fp32},
                      "philox": {"achieved_blocks_per_s": a_int, "peak_blocks_per_s": peaks["philox_blocks"],

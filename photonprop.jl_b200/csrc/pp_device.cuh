@@ -91,16 +91,26 @@ struct Draw4 {
   float u0, u1, u2, u3;
 };
 
-// ((w >> 9) + 1/2) * 2^-23, exact in FP32: 1.m - (1 - 2^-24).
+// ((w >> 9) + 1/2) * 2^-23, exact in FP32: 1.m - (1 - 2^-24).  The mantissa
+// bits (w >> 9) are placed with one integer multiply-add, hi(w * 2^23) +
+// bits(1.0f), which runs on the FMA pipe instead of a shift and an OR on the
+// half-rate ALU pipe.
 __device__ __forceinline__ float u01(uint32_t w) {
-  return __uint_as_float(0x3F800000u | (w >> 9)) - __uint_as_float(0x3F7FFFFFu);
+  uint32_t m;
+  asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(m) : "r"(w), "r"(1u << 23), "r"(0x3F800000u));
+  return __uint_as_float(m) - __uint_as_float(0x3F7FFFFFu);
 }
 
 constexpr uint32_t kKey0 = 0x243F6A88u;  // fixed Philox key (hex digits of pi)
 constexpr uint32_t kKey1 = 0x85A308D3u;
 
-__device__ __forceinline__ Draw4 draw_block(uint32_t seed_lo, uint32_t seed_hi, uint64_t photon, uint32_t block) {
-  uint32_t c[4] = {seed_lo, seed_hi, (uint32_t)photon, (uint32_t)(photon >> 32) | (block << 8)};
+// Counter word 3: photon index bits 32..39 and the block number above them.
+__device__ __forceinline__ uint32_t ctr_word(uint64_t photon, uint32_t block) {
+  return (uint32_t)(photon >> 32) | (block << 8);
+}
+
+__device__ __forceinline__ Draw4 draw_block(uint32_t seed_lo, uint32_t seed_hi, uint64_t photon, uint32_t word3) {
+  uint32_t c[4] = {seed_lo, seed_hi, (uint32_t)photon, word3};
   philox4x32_10(c, kKey0, kKey1);
   return Draw4{u01(c[0]), u01(c[1]), u01(c[2]), u01(c[3])};
 }
@@ -190,17 +200,14 @@ __device__ __forceinline__ void rotate_to_axis(float ox, float oy, float oz, flo
   const float q = fmaf(ox, ny, -oy * nx);
   const float s2 = fmaf(ox, ox, oy * oy);
   const bool up = oz >= 0.f;
-  const float den = up ? 1.f + oz : s2;
+  const float den = up ? 1.f + oz : s2 + 1e-30f;  // finite at o = -e_z, where q = 0
   const float num = up ? 1.f : 1.f - oz;
   const float t = q * num * rcp(den);
   float x = fmaf(nx, oz, fmaf(ox, nz, -oy * t));
-  float y = fmaf(ny, oz, fmaf(oy, nz, ox * t));
-  float z = fmaf(nz, oz, -fmaf(ox, nx, oy * ny));
-  if (den == 0.f) {
-    x = nx;
-    y = -ny;
-    z = -nz;
-  }
+  const float y = fmaf(ny, oz, fmaf(oy, nz, ox * t));
+  const float z = fmaf(nz, oz, -fmaf(ox, nx, oy * ny));
+  // o = -e_z exactly: the formula gives (-n_x, -n_y, -n_z), the reference (n_x, -n_y, -n_z)
+  if (!up && s2 == 0.f) x = nx;
   const float f = fmaf(-0.5f, fmaf(x, x, fmaf(y, y, z * z)), 1.5f);
   rx = x * f;
   ry = y * f;
@@ -222,6 +229,7 @@ struct RunParams {
   double* __restrict__ hist;                  // [n_pairs x hist_bins]
   const DevTables* __restrict__ tables;
   int32_t max_steps;
+  uint32_t ctr_limit;  // (max_steps + 1) << 8: a photon whose next counter word reaches it has ended
   float t_max;
   float hist_t0;
   float inv_bin_width;
@@ -237,7 +245,7 @@ struct Photon {
   float dist;
   float neg_ln2_len;  // -ln2 * scattering length: step = lg2(u) * this
   float max_dist;     // physical mode: path length at t_max
-  int32_t k;          // steps taken
+  uint32_t ctr3;      // Philox counter word of the next event: block (= steps + 1) << 8 | photon bits 32..39
   uint64_t id;
 };
 
@@ -274,6 +282,7 @@ struct EmissionFrame {
   float ox, oy, oz;  // polar axis
   float cpol, spol;  // spol valid only if has_spol
   bool has_spol;
+  bool axis_ez;  // isotropic: the axis is e_z
 };
 
 template <int MODE>
@@ -290,6 +299,7 @@ __device__ __forceinline__ EmissionFrame emission_frame(const DevTables& T, cons
   f.t_emit = pt.w;
   f.has_spol = false;
   f.spol = 0.f;
+  f.axis_ez = emitter == PP_EMITTER_ISOTROPIC;
   if (emitter == PP_EMITTER_ISOTROPIC) {
     f.ox = 0.f;
     f.oy = 0.f;
@@ -328,12 +338,27 @@ __device__ __forceinline__ void polar_direction(float ox, float oy, float oz, fl
 
 __device__ __forceinline__ float sin_from_cos(float c) { return sqrt_a(fmaxf(0.f, fmaf(-c, c, 1.f))); }
 
+// Emission direction of a frame: the isotropic axis is e_z, about which the
+// polar vector needs no rotation; the cone axis is the track.
+__device__ __forceinline__ void emission_direction(const EmissionFrame& f, float u, float& rx, float& ry,
+                                                   float& rz) {
+  const float spol = f.has_spol ? f.spol : sin_from_cos(f.cpol);
+  if (f.axis_ez) {
+    const float ph = fmaf(kTwoPi, u, -kPi);
+    rx = -cos_a(ph) * spol;
+    ry = -sin_a(ph) * spol;
+    rz = f.cpol;
+  } else {
+    polar_direction(f.ox, f.oy, f.oz, f.cpol, spol, u, rx, ry, rz);
+  }
+}
+
 // Emission of photon s.id (block 0): position, direction and the
-// per-wavelength constants; afterwards s.k = 1.
+// per-wavelength constants; afterwards the next event is block 1.
 template <int MODE>
 __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                            const PairCtx& c, Photon& s) {
-  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, 0u);
+  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, ctr_word(s.id, 0u));
   const EmissionFrame f = emission_frame<MODE>(T, P, d);
   s.px = f.px;
   s.py = f.py;
@@ -341,68 +366,56 @@ __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& 
   s.dist = 0.f;
   s.neg_ln2_len = -kLn2 * scattering_length(T, f.wl);
   s.max_dist = (MODE == kPhysical) ? (R.t_max - f.t_emit) * kCVac * rcp(group_index(T, rcp(f.wl))) : 3.0e38f;
-  polar_direction(f.ox, f.oy, f.oz, f.cpol, f.has_spol ? f.spol : sin_from_cos(f.cpol), d.u2, s.dx, s.dy, s.dz);
-  s.k = 1;
+  emission_direction(f, d.u2, s.dx, s.dy, s.dz);
+  s.ctr3 = ctr_word(s.id, 1u);
 }
 
-// Step s.k - 1 (block s.k) of src/photon_prop_cuda.jl:320-376: step length,
+// Step k (block k + 1) of src/photon_prop_cuda.jl:320-376: step length,
 // ray-sphere test, move, Henyey-Greenstein turn.  Returns false when the
 // photon ends; *hit is set when it ends on the sphere (position and path
 // length then at the hit).
 template <int MODE>
 __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c, Photon& s, bool& hit) {
-  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, (uint32_t)s.k);
-  bool alive = true;
+  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, s.ctr3);
   const float step = lg2(d.u0) * s.neg_ln2_len;
   const float ex = s.px - c.tx, ey = s.py - c.ty, ez = s.pz - c.tz;
   const float a = fmaf(s.dz, ez, fmaf(s.dy, ey, s.dx * ex));
   const float pp = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
   const float b = fmaf(a, a, c.r2 - pp);
-  bool move = true;
-  if (b >= 0.f) {
-    const float dd = -a - sqrt_a(b);
-    if (dd > 0.f && dd < step) {
-      move = false;
-      alive = false;
-      if (MODE == kCompat || s.dist + dd <= s.max_dist) {
-        hit = true;
-        s.px = fmaf(dd, s.dx, s.px);
-        s.py = fmaf(dd, s.dy, s.py);
-        s.pz = fmaf(dd, s.dz, s.pz);
-        s.dist += dd;
-      }
-    } else if (MODE == kCompat) {
-      move = false;  // the line meets the sphere outside this step: no move (reference)
-    }
+  // branch-free decisions: the line meets the sphere (b >= 0) at dd ahead
+  const float dd = -a - sqrt_a(fmaxf(b, 0.f));
+  const bool line = b >= 0.f;
+  const bool geo = line && dd > 0.f && dd < step;  // reaches the sphere within this step
+  bool alive, move;
+  if (MODE == kCompat) {
+    hit = geo;
+    move = !line;  // the line meets the sphere outside this step: no move (reference)
+    alive = !geo;
+  } else {
+    hit = geo && s.dist + dd <= s.max_dist;  // arrives inside the time window
+    move = !geo && s.dist + step <= s.max_dist;
+    alive = move;
   }
-  if (move && MODE == kPhysical && s.dist + step > s.max_dist) {
-    move = false;
-    alive = false;
-  }
-  if (move) {
-    s.px = fmaf(step, s.dx, s.px);
-    s.py = fmaf(step, s.dy, s.py);
-    s.pz = fmaf(step, s.dz, s.pz);
-    s.dist += step;
-  }
+  const float len = hit ? dd : (move ? step : 0.f);
+  s.px = fmaf(len, s.dx, s.px);
+  s.py = fmaf(len, s.dy, s.py);
+  s.pz = fmaf(len, s.dz, s.pz);
+  s.dist += len;
   const float cpol = hg_costheta(R.hg, d.u1);
   float rx, ry, rz;
   polar_direction(s.dx, s.dy, s.dz, cpol, sin_from_cos(cpol), d.u2, rx, ry, rz);
-  if (move) {
-    s.dx = rx;
-    s.dy = ry;
-    s.dz = rz;
-  }
-  s.k += 1;
-  if (s.k > R.max_steps) alive = false;  // s.k - 1 steps taken
-  return alive;
+  s.dx = move ? rx : s.dx;
+  s.dy = move ? ry : s.dy;
+  s.dz = move ? rz : s.dz;
+  s.ctr3 += 1u << 8;
+  return alive && s.ctr3 < R.ctr_limit;  // at most max_steps steps
 }
 
-// Emission (s.k == 0) or step event of one photon.
+// Emission (block 0) or step event of one photon.
 template <int MODE>
 __device__ __forceinline__ bool photon_event(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                              const PairCtx& c, Photon& s, bool& hit) {
-  if (s.k == 0) {
+  if (s.ctr3 < (1u << 8)) {
     emit_event<MODE>(T, R, P, c, s);
     return true;
   }
@@ -419,11 +432,11 @@ struct HitValues {
 template <int MODE>
 __device__ __forceinline__ HitValues hit_values(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                                 const PairCtx& c, const Photon& s) {
-  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, 0u);
+  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, ctr_word(s.id, 0u));
   const EmissionFrame f = emission_frame<MODE>(T, P, d);
   HitValues h;
   h.wl = f.wl;
-  polar_direction(f.ox, f.oy, f.oz, f.cpol, f.has_spol ? f.spol : sin_from_cos(f.cpol), d.u2, h.d0x, h.d0y, h.d0z);
+  emission_direction(f, d.u2, h.d0x, h.d0y, h.d0z);
   const float x = 1.f / f.wl;
   if (MODE == kCompat) {
     h.time = s.dist * phase_index(T, x) / kCVac;  // phase velocity (reference)

@@ -62,7 +62,7 @@ __global__ void __launch_bounds__(WARPS * 32) batched_kernel(const RunParams R) 
   bool alive = false;
   Photon s;
   s.id = 0;
-  s.k = 1;
+  s.ctr3 = 1u << 8;
   s.px = s.py = s.pz = s.dx = s.dy = s.dist = s.neg_ln2_len = s.max_dist = 0.f;
   s.dz = 1.f;
   PairCtx c;
@@ -145,8 +145,8 @@ __global__ void __launch_bounds__(WARPS * 32) batched_kernel(const RunParams R) 
         s.neg_ln2_len = b.z;
         s.max_dist = b.w;
         s.dist = 0.f;
-        s.k = 1;
         s.id = ((unsigned long long)__float_as_uint(d.y) << 32) | __float_as_uint(d.x);
+        s.ctr3 = ctr_word(s.id, 1u);
         const int pr = __float_as_int(d.z);
         c = load_pair_ctx(R.pairs + pr, pr);
         alive = true;
@@ -192,13 +192,13 @@ __global__ void __launch_bounds__(512) plain_kernel(const RunParams R, const pp_
        id += stride) {
     Photon s;
     s.id = id;
-    s.k = 0;
+    s.ctr3 = ctr_word(id, 0u);
     s.dx = s.dy = 0.f;
     s.dz = 1.f;
     bool alive = true;
     while (alive) {
       bool hit = false;
-      steps += (s.k > 0);
+      steps += (s.ctr3 >= (1u << 8));
       alive = photon_event<MODE>(T, R, pair_ptr, c, s, hit);
       if (hit) {
         const HitValues h = hit_values<MODE>(T, R, pair_ptr, c, s);
@@ -238,13 +238,13 @@ __global__ void __launch_bounds__(1024) stacks_kernel(const RunParams R, const p
     if (*(volatile int*)&cursor > ix_offset + stack_len - safe_margin) break;
     Photon s;
     s.id = g + (unsigned long long)i * G;
-    s.k = 0;
+    s.ctr3 = ctr_word(s.id, 0u);
     s.dx = s.dy = 0.f;
     s.dz = 1.f;
     bool alive = true;
     while (alive) {
       bool hit = false;
-      steps += (s.k > 0);
+      steps += (s.ctr3 >= (1u << 8));
       alive = photon_event<MODE>(T, R, pair_ptr, c, s, hit);
       if (hit) {
         const HitValues h = hit_values<MODE>(T, R, pair_ptr, c, s);
@@ -460,6 +460,7 @@ static __host__ ppd::RunParams to_params(const LaunchArgs& a) {
   R.hist = a.hist;
   R.tables = reinterpret_cast<const ppd::DevTables*>(a.tables);
   R.max_steps = a.opts.max_steps;
+  R.ctr_limit = ((uint32_t)a.opts.max_steps + 1u) << 8;
   R.t_max = a.opts.t_max;
   R.hist_t0 = a.opts.hist_t0;
   R.inv_bin_width = a.opts.hist_bin_width > 0.f ? 1.f / a.opts.hist_bin_width : 0.f;

@@ -27,3 +27,13 @@ def op_counts(steps, photons_iso, photons_cone):
     fp32 = steps * FP32_PER_STEP + photons_iso * FP32_PER_PHOTON[0] + photons_cone * FP32_PER_PHOTON[1]
     blocks = steps * PHILOX_PER_STEP + (photons_iso + photons_cone) * PHILOX_PER_PHOTON
     return mufu, fp32, blocks
+
+
+# DRAM traffic of the batched kernel per photon, measured with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) on one launch of 2.524e8
+# photons (512 mixed pairs, <= 1e6 photons each): 113.7 KB read, 0 B written.
+# Hit records and FP64 histogram reductions stay in L2 during a launch, so
+# the traffic grows with the photon count; bench.py scales it to its launch.
+NCU_DRAM_BYTES_PER_PHOTON = 113.664e3 / 252387747
+# Issue slots busy in the same capture (smsp__issue_active).
+NCU_ISSUE_ACTIVE = 0.790
