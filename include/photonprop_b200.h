@@ -52,7 +52,8 @@ enum { PP_SPECTRUM_CHERENKOV = 0, PP_SPECTRUM_MONOCHROMATIC = 1 };
 enum {
   PP_OPT_PMT_WEIGHT = 1u, /* multiply hit weights by the PMT acceptance */
   PP_OPT_NORMALIZE = 2u,  /* divide each pair's histogram by its photon count */
-  PP_OPT_NO_HITS = 4u     /* accumulate statistics only; write no hit records */
+  PP_OPT_NO_HITS = 4u,    /* accumulate statistics only; write no hit records */
+  PP_OPT_COMPACT_HITS = 8u /* write pp_hit32 records instead of pp_hit */
 };
 
 #define PP_MAX_KNOTS 64
@@ -139,6 +140,17 @@ typedef struct {
   uint32_t pair;    /* index of the pair in the call */
   uint64_t photon;  /* photon index within the pair */
 } pp_hit;
+
+/* Compact hit record (PP_OPT_COMPACT_HITS), 32 bytes: what the serving loop
+ * returns.  photon_lo holds the low 32 bits of the photon index. */
+typedef struct {
+  float pos[3];
+  float time;
+  float weight;
+  float wavelength;
+  uint32_t photon_lo;
+  uint32_t pair;
+} pp_hit32;
 
 typedef struct pp_ctx pp_ctx;
 
@@ -256,6 +268,52 @@ PP_API pp_status pp_cuda_propagate_photons(pp_ctx* ctx, float* d_out_positions,
                                     int32_t n_blocks, int32_t threads,
                                     const pp_pair* source_target, const pp_run_opts* opts,
                                     void* stream);
+
+/* ---- serving: continuous batching ----------------------------------------- */
+/* A request is a list of pairs.  A scheduler thread admits waiting requests
+ * while their hit buffers fit the HBM budget (bytes_per_hit per expected hit)
+ * and an in-flight slot is free, packs every admitted request into one batched
+ * launch on that slot's stream, and keeps up to max_inflight batches on the
+ * device at once; requests that arrive while batches run join the next batch
+ * as slots and memory free up.  The medium tables and the kernels' RNG (a
+ * counter-based stream, no state) are resident in the context.  Results are
+ * the same as a request alone: a pair's photons depend only on its seed. */
+typedef struct {
+  int32_t max_inflight;        /* batches on the device at once (streams); 0 = 2 */
+  int32_t max_pairs_per_batch; /* 0 = 4096 */
+  int64_t hbm_budget_bytes;    /* admission budget; 0 = 40 GiB */
+  int32_t bytes_per_hit;       /* admission bytes per expected hit; 0 = 32 (pp_hit32) */
+  float hit_safety;            /* hit slots per expected hit; 0 = 4 */
+  int32_t max_queued;          /* waiting requests before submit says PP_ERR_BUSY; 0 = 100000 */
+  int32_t reserved;
+  pp_run_opts opts;            /* physics and histogram options of every request */
+} pp_server_config;
+
+typedef struct pp_server pp_server;
+
+typedef struct {
+  int64_t submitted, completed, batches, pairs, in_flight_batches, waiting;
+  int64_t reserved_bytes;
+  double photons;
+} pp_server_counters;
+
+/* Starts the scheduler thread on ctx's device; the context must outlive the server. */
+PP_API pp_status pp_server_create(pp_ctx* ctx, const pp_server_config* cfg, pp_server** out);
+/* Stops the scheduler after the batches on the device finish. */
+PP_API void pp_server_destroy(pp_server* s);
+/* Queues a request (the pairs are copied); never blocks.  PP_ERR_BUSY when
+ * max_queued requests wait, PP_ERR_ARG when it could never fit the budget. */
+PP_API pp_status pp_server_submit(pp_server* s, const pp_pair* pairs, int32_t n_pairs, uint64_t* request_id);
+/* Waits up to timeout_s for a request (PP_ERR_TIMEOUT after that). */
+PP_API pp_status pp_server_wait(pp_server* s, uint64_t request_id, double timeout_s);
+/* Copies a finished request's results out and forgets it: compact hits (up
+ * to hit_capacity; *n_hits = its hits in the buffer), stats [n_pairs x 8],
+ * hist [n_pairs x bins], latency = completion - submission in seconds.
+ * PP_ERR_STATE if the request is not finished; PP_ERR_OVERFLOW if some of its
+ * hits did not fit the batch's hit buffer (stats and hist are complete). */
+PP_API pp_status pp_server_result(pp_server* s, uint64_t request_id, pp_hit32* hits, int64_t hit_capacity,
+                                  int64_t* n_hits, double* stats, double* hist, double* latency_s);
+PP_API pp_status pp_server_get_counters(pp_server* s, pp_server_counters* out);
 
 /* ---- tuning and diagnostics ---------------------------------------------- */
 /* Times the batched kernel over (block size, blocks per SM, chunk) on a

@@ -287,6 +287,8 @@ pp::LaunchArgs base_args(pp_ctx* c, const pp_run_opts* o) {
 
 bool aligned(const void* p, uintptr_t a) { return ((uintptr_t)p % a) == 0; }
 
+size_t hit_bytes(const pp_run_opts* o) { return (o->flags & PP_OPT_COMPACT_HITS) ? sizeof(pp_hit32) : sizeof(pp_hit); }
+
 pp_status alloc_fail(pp_ctx* c, cudaError_t e, const char* what) {
   if (e == cudaErrorMemoryAllocation) {
     cudaGetLastError();
@@ -533,7 +535,7 @@ pp_status pp_propagate(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const p
   *n_hits = total;
   const int64_t ncopy = std::min<int64_t>(total, cap);
   if (ncopy > 0 && !(opts->flags & PP_OPT_NO_HITS) &&
-      (e = cudaMemcpyAsync(hits, c->hits.p, (size_t)ncopy * sizeof(pp_hit), cudaMemcpyDeviceToHost, s)))
+      (e = cudaMemcpyAsync(hits, c->hits.p, (size_t)ncopy * hit_bytes(opts), cudaMemcpyDeviceToHost, s)))
     return c->cuda_fail(e, "copy hits");
   if (n_pairs > 0 &&
       (e = cudaMemcpyAsync(stats, c->stats.p, (size_t)n_pairs * PP_STATS * sizeof(double), cudaMemcpyDeviceToHost, s)))
@@ -631,8 +633,8 @@ pp_status pp_propagate_plain(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, c
     const int64_t nh = (int64_t)cnt[0];
     const int64_t ncopy = std::min<int64_t>(nh, room);
     if (ncopy > 0 && !(opts->flags & PP_OPT_NO_HITS) &&
-        (e = cudaMemcpyAsync(hits + std::min(total, cap), c->hits.p, (size_t)ncopy * sizeof(pp_hit),
-                             cudaMemcpyDeviceToHost, c->stream)))
+        (e = cudaMemcpyAsync(reinterpret_cast<char*>(hits) + (size_t)std::min(total, cap) * hit_bytes(opts), c->hits.p,
+                             (size_t)ncopy * hit_bytes(opts), cudaMemcpyDeviceToHost, c->stream)))
       return c->cuda_fail(e, "copy hits");
     if ((e = cudaMemcpyAsync(stats + p * PP_STATS, c->stats.p, PP_STATS * sizeof(double), cudaMemcpyDeviceToHost,
                              c->stream)))
@@ -817,6 +819,42 @@ pp_status pp_autotune(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Batched propagation with caller-owned work-queue scratch and no graph: the
+// serving loop runs several batches at once, each with its own scratch.
+namespace pp {
+pp_status propagate_with_scratch(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs, const pp_run_opts* opts,
+                                 void* d_hits, int64_t cap, uint64_t* d_counters, double* d_stats,
+                                 double* d_hist, unsigned long long* d_offsets, unsigned long long* d_queue,
+                                 cudaStream_t stream) {
+  if (!c) return PP_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  pp_status st = validate_opts(c, opts);
+  if (st) return st;
+  DeviceGuard guard(c->device);
+  int grid, block;
+  uint32_t chunk;
+  resolve_launch(c, *opts, grid, block, chunk);
+  pp::LaunchArgs a = base_args(c, opts);
+  a.pairs = d_pairs;
+  a.n_pairs = n_pairs;
+  a.queue = d_queue;
+  a.chunk_offsets = d_offsets;
+  a.chunk = chunk;
+  a.hits = static_cast<pp_hit*>(d_hits);
+  a.hit_cap = (unsigned long long)cap;
+  a.counters = reinterpret_cast<unsigned long long*>(d_counters);
+  a.stats = d_stats;
+  a.hist = opts->hist_bins > 0 ? d_hist : nullptr;
+  const cudaError_t e = enqueue_batched(c, a, grid, block, stream);
+  if (e) return c->cuda_fail(e, "batched launch");
+  return PP_OK;
+}
+
+int ctx_device(const pp_ctx* c) { return c->device; }
+int ctx_sm_count(const pp_ctx* c) { return c->sm_count; }
+}  // namespace pp
 
 // ---------------------------------------------------------------------------
 // Allocation-free batched propagation (pp_propagate_device_noalloc).

@@ -477,12 +477,19 @@ __device__ __forceinline__ void record_hit(const RunParams& R, const PairCtx& c,
   if (R.flags & PP_OPT_NO_HITS) return;
   const unsigned long long idx = base + rank;
   if (idx < R.hit_cap) {
-    float4* dst = reinterpret_cast<float4*>(R.hits + idx);
-    dst[0] = make_float4(s.px, s.py, s.pz, h.time);
-    dst[1] = make_float4(h.d0x, h.d0y, h.d0z, h.weight);
-    dst[2] = make_float4(s.dx, s.dy, s.dz, h.wl);
-    dst[3] = make_float4(s.dist, __uint_as_float((uint32_t)c.index + R.pair_base),
-                         __uint_as_float((uint32_t)s.id), __uint_as_float((uint32_t)(s.id >> 32)));
+    if (R.flags & PP_OPT_COMPACT_HITS) {
+      float4* dst = reinterpret_cast<float4*>(reinterpret_cast<pp_hit32*>(R.hits) + idx);
+      dst[0] = make_float4(s.px, s.py, s.pz, h.time);
+      dst[1] = make_float4(h.weight, h.wl, __uint_as_float((uint32_t)s.id),
+                           __uint_as_float((uint32_t)c.index + R.pair_base));
+    } else {
+      float4* dst = reinterpret_cast<float4*>(R.hits + idx);
+      dst[0] = make_float4(s.px, s.py, s.pz, h.time);
+      dst[1] = make_float4(h.d0x, h.d0y, h.d0z, h.weight);
+      dst[2] = make_float4(s.dx, s.dy, s.dz, h.wl);
+      dst[3] = make_float4(s.dist, __uint_as_float((uint32_t)c.index + R.pair_base),
+                           __uint_as_float((uint32_t)s.id), __uint_as_float((uint32_t)(s.id >> 32)));
+    }
   } else {
     atomicOr(R.counters + 2, 1ull);
   }

@@ -52,6 +52,14 @@ int batched_max_blocks_per_sm(int mode, int block);
 int plain_max_blocks_per_sm(int mode, int block);
 cudaError_t run_peaks(int sm_count, double* fp32, double* mufu, double* iops);
 
+// batched launch with caller-owned scratch, direct launches (pp_capi.cu)
+pp_status propagate_with_scratch(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs, const pp_run_opts* opts,
+                                 void* d_hits, int64_t cap, uint64_t* d_counters, double* d_stats,
+                                 double* d_hist, unsigned long long* d_offsets, unsigned long long* d_queue,
+                                 cudaStream_t stream);
+int ctx_device(const pp_ctx* c);
+int ctx_sm_count(const pp_ctx* c);
+
 // host physics (pp_host_physics.cpp)
 void medium_coeffs(const pp_medium_desc* m, double out[11]);
 void default_abs_table(double* wl, double* len, int* n);

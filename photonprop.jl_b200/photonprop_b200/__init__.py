@@ -16,6 +16,7 @@ from .propagation import (PropagationResult, Propagator, RunOptions, cuda_propag
                           propagate_distance)
 from .spectrum import CherenkovSpectrum, Monochromatic, Spectrum
 from . import batches
+from . import serving
 
 
 def build(force=False):

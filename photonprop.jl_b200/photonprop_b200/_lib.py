@@ -20,7 +20,7 @@ STATUS_NAMES = {0: "PP_OK", 1: "PP_ERR_ARG", 2: "PP_ERR_OOM", 3: "PP_ERR_OVERFLO
 MODE_COMPAT, MODE_PHYSICAL = 0, 1
 EMITTER_ISOTROPIC, EMITTER_CHERENKOV_CONE = 0, 1
 SPECTRUM_CHERENKOV, SPECTRUM_MONOCHROMATIC = 0, 1
-OPT_PMT_WEIGHT, OPT_NORMALIZE, OPT_NO_HITS = 1, 2, 4
+OPT_PMT_WEIGHT, OPT_NORMALIZE, OPT_NO_HITS, OPT_COMPACT_HITS = 1, 2, 4, 8
 MAX_KNOTS, MAX_ABS, MAX_PMT, N_STATS = 64, 32, 256, 8
 NOALLOC_MAX_PAIRS = 65536
 
@@ -35,6 +35,11 @@ HIT_DTYPE = np.dtype([
     ("dir", "<f4", 3), ("wavelength", "<f4"), ("dist", "<f4"), ("pair", "<u4"),
     ("photon", "<u8")])
 assert HIT_DTYPE.itemsize == 64
+
+HIT32_DTYPE = np.dtype([
+    ("pos", "<f4", 3), ("time", "<f4"), ("weight", "<f4"), ("wavelength", "<f4"), ("photon_lo", "<u4"),
+    ("pair", "<u4")])
+assert HIT32_DTYPE.itemsize == 32
 
 
 class MediumDesc(ctypes.Structure):
@@ -62,6 +67,19 @@ class RunOpts(ctypes.Structure):
                 ("flags", ctypes.c_uint32), ("block_size", ctypes.c_int32),
                 ("blocks_per_sm", ctypes.c_int32), ("chunk_photons", ctypes.c_int32),
                 ("reserved", ctypes.c_int32)]
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("max_inflight", ctypes.c_int32), ("max_pairs_per_batch", ctypes.c_int32),
+                ("hbm_budget_bytes", ctypes.c_int64), ("bytes_per_hit", ctypes.c_int32),
+                ("hit_safety", ctypes.c_float), ("max_queued", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("opts", RunOpts)]
+
+
+class ServerCounters(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_int64), ("completed", ctypes.c_int64), ("batches", ctypes.c_int64),
+                ("pairs", ctypes.c_int64), ("in_flight_batches", ctypes.c_int64), ("waiting", ctypes.c_int64),
+                ("reserved_bytes", ctypes.c_int64), ("photons", ctypes.c_double)]
 
 
 class PPError(RuntimeError):
@@ -106,6 +124,13 @@ _SIGS = [
                                                  _I64, _VP, _VP, _VP, _VP]),
     ("pp_cuda_propagate_photons", ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _I32, _I32, _I32,
                                                  _VP, ctypes.POINTER(RunOpts), _VP]),
+    ("pp_server_create", ctypes.c_int, [_VP, ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
+    ("pp_server_destroy", None, [_VP]),
+    ("pp_server_submit", ctypes.c_int, [_VP, _VP, _I32, ctypes.POINTER(ctypes.c_uint64)]),
+    ("pp_server_wait", ctypes.c_int, [_VP, ctypes.c_uint64, _D]),
+    ("pp_server_result", ctypes.c_int, [_VP, ctypes.c_uint64, _VP, _I64, ctypes.POINTER(_I64), _VP, _VP,
+                                        ctypes.POINTER(_D)]),
+    ("pp_server_get_counters", ctypes.c_int, [_VP, ctypes.POINTER(ServerCounters)]),
     ("pp_autotune", ctypes.c_int, [_VP, _VP, _I64, ctypes.POINTER(RunOpts), ctypes.c_char_p,
                                    ctypes.POINTER(RunOpts), ctypes.POINTER(_D)]),
     ("pp_device_eval", ctypes.c_int, [_VP, _I32, _VP, _VP, _I64]),
