@@ -54,6 +54,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
+    ap.add_argument("--serving-seconds", type=float, default=10.0,
+                    help="length of the serving sample in the default run (0 = skip)")
+    ap.add_argument("--workload", choices=["batch", "serving"], default="batch")
     ap.add_argument("--max-photons", type=int, default=0,
                     help="cap photons per pair (small profiling cases; 0 = no cap)")
     return ap.parse_args()
@@ -148,6 +151,43 @@ def cpu_baseline(batch, target_seconds, run_kw):
     return {"value": photons / dt, "unit": UNIT, "cores": cores, "kind": "port",
             "sample": f"first {lim} photons of each of the {len(batch)} pairs ({photons:.3e} photons, "
                       f"{dt:.1f} s), FP64 oracle, OpenMP {cores} threads"}
+
+
+def run_serving(prop, seconds, seed=0, rate_hz=200.0):
+    """Open-loop Poisson stream (rate_hz, 1-64 pairs per request, 1e4-1e6
+    photons per pair) through the continuous-batching server and through the
+    one-launch-per-request loop on the same arrivals."""
+    from photonprop_b200 import serving
+    arrivals, reqs = serving.requests(rate_hz=rate_hz, duration_s=seconds, seed=seed)
+    opts = serving.RunOptions(mode="physical", g=0.95, t_max=1000.0, hist_bins=1000)
+    with serving.Server(prop, opts) as srv:
+        w_arr, w_req = serving.requests(rate_hz=rate_hz, duration_s=min(1.0, seconds), seed=seed + 99)
+        serving.run_open_loop(srv, w_arr, w_req)  # warm-up
+        out, _ = serving.run_open_loop(srv, arrivals, reqs)
+        out["batches"] = srv.counters()["batches"]
+    plain = serving.run_plain_loop(prop, opts, arrivals, reqs)
+    return {"rate_hz": rate_hz, "seconds": seconds, "continuous_batching": out, "plain_loop": plain,
+            "what": "request latency = completion - arrival (host clock); photons/s over the stream"}
+
+
+def run_serving_workload(args):
+    """--workload serving: the full serving configuration on one GPU."""
+    import torch
+    import photonprop_b200 as pp
+    torch.cuda.set_device(0)
+    medium = pp.make_seawater(35.0, 2.0)
+    spec = pp.CherenkovSpectrum((300.0, 800.0), 20, medium)
+    with pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=0) as prop:
+        r = run_serving(prop, args.serving_seconds, seed=args.seed)
+    cb = r["continuous_batching"]
+    line = {"metric": "serving photons/s; p50/p99/p99.9 request latency", "value": cb["photons_per_s"],
+            "unit": UNIT, "n_gpus": 1, "latency_ms": {k: cb[k] for k in ("p50_ms", "p99_ms", "p99.9_ms")},
+            "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": f"Poisson {r['rate_hz']} req/s for {r['seconds']} s, 1-64 pairs/request, "
+                                   "photons/pair log-uniform [1e4,1e6], mixed emitters, 40 GB HBM admission "
+                                   "budget at 32 B per expected hit"},
+            "serving": r}
+    print(json.dumps(line), flush=True)
 
 
 def run_reference(args):
@@ -342,6 +382,10 @@ def run_ours(args):
         d2h += 32 + min(nh, cap) * 64 + n_pairs * 8 * 8 + n_pairs * bins * 8
     e2e_value = photons_all / reduce(e2e_t, MAX)
 
+    serve = None
+    if args.serving_seconds > 0:
+        serve = run_serving(prop, args.serving_seconds, seed=args.seed + rank)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(batches[W], args.cpu_seconds, RUN_KW)
@@ -377,6 +421,7 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n_pairs * 80,
                 "d2h_bytes_per_step": int(d2h / K)},
         "plain": plain,
+        "serving": serve,
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
@@ -394,6 +439,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "serving":
+        run_serving_workload(args)
     else:
         run_ours(args)
 

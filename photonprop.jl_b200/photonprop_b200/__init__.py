@@ -17,6 +17,7 @@ from .propagation import (PropagationResult, Propagator, RunOptions, cuda_propag
 from .spectrum import CherenkovSpectrum, Monochromatic, Spectrum
 from . import batches
 from . import serving
+from . import parallel
 
 
 def build(force=False):
