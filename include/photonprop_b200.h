@@ -315,6 +315,46 @@ PP_API pp_status pp_server_result(pp_server* s, uint64_t request_id, pp_hit32* h
                                   int64_t* n_hits, double* stats, double* hist, double* latency_s);
 PP_API pp_status pp_server_get_counters(pp_server* s, pp_server_counters* out);
 
+/* ---- learned surrogate ------------------------------------------------------ */
+/* MLP 4 -> 128 -> 128 -> 128 -> 5 (GELU) replacing the reference's Flux
+ * fits (src/modelling.jl:202-267).  Inputs per query (raw): log10 distance,
+ * cos(emitter-target angle), log10 photons, emitter flag.  Outputs: ln(mu/N)
+ * (mu = expected weighted hits), logit w, ln a1, ln a2, ln theta of a
+ * two-component Gamma mixture w G(a1, theta) + (1-w) G(a2, theta) of the time
+ * residual; `physical` returns (mu, w, a1, a2, theta) instead.  BF16 weights
+ * and activations, FP32 accumulation; the 128 x 128 layers run on tcgen05
+ * tensor cores.  Parameters: N_PARAMS FP32 values in the order W1[128][4],
+ * b1, W2[128][128], b2, W3[128][128], b3, W4[5][128], b4. */
+typedef struct pp_mlp pp_mlp;
+PP_API pp_status pp_mlp_create(int device, uint64_t seed, pp_mlp** out);
+PP_API void pp_mlp_destroy(pp_mlp* m);
+PP_API const char* pp_mlp_last_error(const pp_mlp* m);
+PP_API int32_t pp_mlp_num_params(void);
+PP_API pp_status pp_mlp_get_params(pp_mlp* m, float* out);
+PP_API pp_status pp_mlp_set_params(pp_mlp* m, const float* in);
+/* Feature and target standardisation: x' = (x - mean) / std, y = y' std + mean. */
+PP_API pp_status pp_mlp_set_normalization(pp_mlp* m, const float* x_mean, const float* x_std, const float* y_mean,
+                                          const float* y_std);
+PP_API pp_status pp_mlp_get_normalization(pp_mlp* m, float* out18);
+/* Inference on device buffers: x [n][4], out [5][n]. */
+PP_API pp_status pp_mlp_forward(pp_mlp* m, const float* d_x, float* d_out, int64_t n, int32_t physical,
+                                void* stream);
+/* One Adam step (lr > 0) on standardised device data xn [n][4], yt [n][5],
+ * mask [n][5] with masked-MSE loss; *loss_out = mean loss; grad_out (host,
+ * N_PARAMS) receives the gradients if not NULL (lr = 0: gradients only). */
+PP_API pp_status pp_mlp_train_step(pp_mlp* m, const float* d_xn, const float* d_yt, const float* d_mask, int64_t n,
+                                   float lr, float* loss_out, float* grad_out);
+/* One 128 x 128 x 128 BF16 GEMM (c = a b^T, row-major) through the tcgen05
+ * path: a check of the tensor-core descriptors. */
+PP_API pp_status pp_mlp_gemm_selftest(int device, const uint16_t* a_bf16, const uint16_t* b_bf16, float* c);
+
+/* Fits w G(a1, theta) + (1 - w) G(a2, theta) to each of n histograms
+ * (device, FP64 [n][bins], bin b centred at t0 + (b + 1/2) bin_width) as a
+ * function of t - tshift[i] by weighted EM (iters iterations); d_out [n][5] =
+ * w, a1 <= a2, theta, mean log-likelihood (NaN for empty histograms). */
+PP_API pp_status pp_gamma_mixture_fit(const double* d_hist, int64_t n, int32_t bins, float t0, float bin_width,
+                                      const float* d_tshift, float* d_out, int32_t iters, void* stream);
+
 /* ---- tuning and diagnostics ---------------------------------------------- */
 /* Times the batched kernel over (block size, blocks per SM, chunk) on a
  * sample of `pairs` and stores the best in the context (and in the cache

@@ -18,6 +18,7 @@ from .spectrum import CherenkovSpectrum, Monochromatic, Spectrum
 from . import batches
 from . import serving
 from . import parallel
+from . import surrogate
 
 
 def build(force=False):

@@ -131,6 +131,19 @@ _SIGS = [
     ("pp_server_result", ctypes.c_int, [_VP, ctypes.c_uint64, _VP, _I64, ctypes.POINTER(_I64), _VP, _VP,
                                         ctypes.POINTER(_D)]),
     ("pp_server_get_counters", ctypes.c_int, [_VP, ctypes.POINTER(ServerCounters)]),
+    ("pp_mlp_create", ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.POINTER(_VP)]),
+    ("pp_mlp_destroy", None, [_VP]),
+    ("pp_mlp_last_error", ctypes.c_char_p, [_VP]),
+    ("pp_mlp_num_params", ctypes.c_int32, []),
+    ("pp_mlp_get_params", ctypes.c_int, [_VP, _VP]),
+    ("pp_mlp_set_params", ctypes.c_int, [_VP, _VP]),
+    ("pp_mlp_set_normalization", ctypes.c_int, [_VP, _VP, _VP, _VP, _VP]),
+    ("pp_mlp_get_normalization", ctypes.c_int, [_VP, _VP]),
+    ("pp_mlp_forward", ctypes.c_int, [_VP, _VP, _VP, _I64, _I32, _VP]),
+    ("pp_mlp_train_step", ctypes.c_int, [_VP, _VP, _VP, _VP, _I64, ctypes.c_float, ctypes.POINTER(ctypes.c_float),
+                                         _VP]),
+    ("pp_mlp_gemm_selftest", ctypes.c_int, [ctypes.c_int, _VP, _VP, _VP]),
+    ("pp_gamma_mixture_fit", ctypes.c_int, [_VP, _I64, _I32, ctypes.c_float, ctypes.c_float, _VP, _VP, _I32, _VP]),
     ("pp_autotune", ctypes.c_int, [_VP, _VP, _I64, ctypes.POINTER(RunOpts), ctypes.c_char_p,
                                    ctypes.POINTER(RunOpts), ctypes.POINTER(_D)]),
     ("pp_device_eval", ctypes.c_int, [_VP, _I32, _VP, _VP, _I64]),

@@ -1,0 +1,138 @@
+"""The learned surrogate: tensor-core GEMM path, forward and backward kernels
+against the FP64 oracle, the Gamma-mixture fit, training and the MC
+fallback.  Tolerances: GEMM rtol 1e-5 (exact BF16 products, FP32 sums);
+network outputs |dy| <= 2e-2 (1 + |y|) (BF16 activations); gradients:
+relative L2 error per parameter block <= 2e-2."""
+import numpy as np
+import pytest
+
+import photonprop_b200 as pp
+from photonprop_b200 import surrogate as sg
+from oracle import mlp as omlp
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16_bits(x):
+    a = np.asarray(x, dtype=np.float32)
+    b = a.view(np.uint32).astype(np.uint64)
+    return (((b + 0x7FFF + ((b >> 16) & 1)) >> 16) & 0xFFFF).astype(np.uint16)
+
+
+def test_tcgen05_gemm_selftest():
+    rng = np.random.default_rng(0)
+    a = rng.normal(size=(128, 128)).astype(np.float32)
+    b = rng.normal(size=(128, 128)).astype(np.float32)
+    ab, bb = _bf16_bits(a), _bf16_bits(b)
+    c = sg.gemm_selftest(ab, bb)
+    a64 = omlp.bf16(a)
+    b64 = omlp.bf16(b)
+    np.testing.assert_allclose(c, a64 @ b64.T, rtol=1e-5, atol=1e-4)
+
+
+def _net_with_norm(seed=1):
+    net = sg.MLP(0, seed)
+    net.set_normalization(np.zeros(4), np.ones(4), np.zeros(5), np.ones(5))
+    return net
+
+
+def test_forward_matches_oracle():
+    import torch
+    net = _net_with_norm()
+    p = net.get_params().astype(np.float64)
+    rng = np.random.default_rng(1)
+    n = 1000  # 8 tiles, the last one partial
+    x = rng.normal(size=(n, 4)).astype(np.float32)
+    d_x = torch.from_numpy(x).cuda()
+    d_o = torch.empty((5, n), dtype=torch.float32, device="cuda")
+    net.forward(d_x, d_o, n, physical=False)
+    y = d_o.cpu().numpy().T
+    ref, _ = omlp.forward(p, x.astype(np.float64))
+    assert np.all(np.abs(y - ref) <= 2e-2 * (1 + np.abs(ref))), np.abs(y - ref).max()
+    net.close()
+
+
+def test_gradients_match_oracle():
+    import torch
+    net = _net_with_norm(seed=3)
+    p = net.get_params().astype(np.float64)
+    rng = np.random.default_rng(2)
+    n = 300  # 3 tiles, the last one partial
+    x = rng.normal(size=(n, 4)).astype(np.float32)
+    yt = rng.normal(size=(n, 5)).astype(np.float32)
+    mask = (rng.uniform(size=(n, 5)) < 0.8).astype(np.float32)
+    loss, g = net.train_step(torch.from_numpy(x).cuda(), torch.from_numpy(yt).cuda(), torch.from_numpy(mask).cuda(),
+                             n, 0.0, want_grads=True)
+    ref_loss, ref_g = omlp.loss_and_grads(p, x.astype(np.float64), yt.astype(np.float64), mask.astype(np.float64))
+    assert loss == pytest.approx(ref_loss, rel=1e-2)
+    off = 0
+    for name, shape in omlp.SIZES:
+        k = int(np.prod(shape))
+        a, b = g[off:off + k].astype(np.float64), ref_g[off:off + k]
+        err = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+        print(name, err)
+        assert err < 2e-2, (name, err)
+        off += k
+    net.close()
+
+
+def test_adam_step_reduces_loss():
+    import torch
+    net = _net_with_norm(seed=4)
+    rng = np.random.default_rng(3)
+    n = 4096
+    x = rng.normal(size=(n, 4)).astype(np.float32)
+    yt = np.stack([np.sin(x[:, 0]) + x[:, 1] * x[:, 2], x[:, 3] ** 2 - 1, np.cos(x[:, 1]), x[:, 0] * 0.5,
+                   np.tanh(x[:, 2])], axis=1).astype(np.float32)
+    mask = np.ones((n, 5), dtype=np.float32)
+    d = [torch.from_numpy(a).cuda() for a in (x, yt, mask)]
+    losses = [net.train_step(*d, n, 3e-3)[0] for _ in range(300)]
+    assert losses[-1] < 0.2 * losses[0], (losses[0], losses[-1])
+    net.close()
+
+
+def test_gamma_mixture_fit_recovers_parameters():
+    import torch
+    from scipy import stats as st
+    w, a1, a2, th = 0.35, 2.5, 12.0, 3.0
+    edges = np.arange(0.0, 301.0, 1.0)
+    cdf = w * st.gamma.cdf(edges, a1, scale=th) + (1 - w) * st.gamma.cdf(edges, a2, scale=th)
+    h = np.diff(cdf)[None, :] * 1e5
+    d_h = torch.from_numpy(h).cuda()
+    d_ts = torch.zeros(1, dtype=torch.float32, device="cuda")
+    d_o = torch.zeros((1, 5), dtype=torch.float32, device="cuda")
+    pp._lib.check(pp._lib.load().pp_gamma_mixture_fit(d_h.data_ptr(), 1, 300, 0.0, 1.0, d_ts.data_ptr(),
+                                                       d_o.data_ptr(), 200, None))
+    o = d_o.cpu().numpy()[0]
+    np.testing.assert_allclose(o[:4], [w, a1, a2, th], rtol=0.05)
+
+
+def test_surrogate_trains_and_falls_back_to_mc(propagator):
+    opts = pp.RunOptions(mode="physical", t_max=1000.0, hist_bins=1000)
+    train = sg.mc_dataset(propagator, sg.training_pairs(16384, 1_000_000, seed=11, d_min=2.0, d_max=10.0), opts)
+    test = sg.mc_dataset(propagator, sg.training_pairs(1024, 1_000_000, seed=12, d_min=2.0, d_max=10.0), opts)
+    s = sg.Surrogate(propagator, opts, seed=5)
+    losses = s.fit(train, epochs=60, batch=1024, lr=2e-3)
+    print("loss", losses[0], losses[-1])
+    assert losses[-1] < 0.7 * losses[0], losses
+    raw = s.predict_features(test.x, physical=False)
+    for j in range(5):
+        m = test.mask[:, j] > 0
+        r2 = 1 - np.mean((raw[m, j] - test.y[m, j]) ** 2) / np.var(test.y[m, j])
+        print("output", j, "held-out R^2", r2, "n", m.sum())
+    # expected hits on held-out pairs whose MC value is known to 3 %
+    good = test.hits >= 1000
+    pred = s.predict_features(test.x[good], physical=True)
+    rel = np.abs(pred[:, 0] - test.mu[good]) / test.mu[good]
+    print("pairs", good.sum(), "median rel err", np.median(rel), "within 5%", np.mean(rel < 0.05))
+    assert good.sum() > 50 and np.median(rel) < 0.10
+    # the photon count scales the expected hits exactly
+    x = test.x[good][:8].copy()
+    x[:, 2] = 5.0
+    np.testing.assert_allclose(s.predict_features(x)[:, 0], pred[:8, 0] / 10.0, rtol=1e-5)
+    # outside the trained distance range the MC kernel answers
+    far = sg.training_pairs(4, 200_000, seed=13, d_min=100.0, d_max=120.0)
+    out, used_mc = s.predict(far)
+    assert used_mc.all()
+    mc = sg.mc_dataset(propagator, far, opts, min_hits_mu=0, min_hits_fit=0)
+    np.testing.assert_allclose(out[:, 0], mc.mu, rtol=1e-9)
