@@ -56,7 +56,14 @@ def parse():
     ap.add_argument("--no-tune", action="store_true")
     ap.add_argument("--serving-seconds", type=float, default=10.0,
                     help="length of the serving sample in the default run (0 = skip)")
-    ap.add_argument("--workload", choices=["batch", "serving"], default="batch")
+    ap.add_argument("--serving-rate", type=float, default=200.0, help="request arrival rate, Hz")
+    ap.add_argument("--workload", choices=["batch", "serving", "surrogate", "surrogate-infer"], default="batch")
+    ap.add_argument("--train-pairs", type=int, default=200_000)
+    ap.add_argument("--test-pairs", type=int, default=20_000)
+    ap.add_argument("--epochs", type=int, default=400)
+    ap.add_argument("--train-distance", choices=["uniform", "loguniform"], default="loguniform",
+                    help="distance law of the surrogate's training pairs (held-out pairs: uniform)")
+    ap.add_argument("--full-weight-hits", type=float, default=1000.0)
     ap.add_argument("--max-photons", type=int, default=0,
                     help="cap photons per pair (small profiling cases; 0 = no cap)")
     return ap.parse_args()
@@ -178,7 +185,7 @@ def run_serving_workload(args):
     medium = pp.make_seawater(35.0, 2.0)
     spec = pp.CherenkovSpectrum((300.0, 800.0), 20, medium)
     with pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=0) as prop:
-        r = run_serving(prop, args.serving_seconds, seed=args.seed)
+        r = run_serving(prop, args.serving_seconds, seed=args.seed, rate_hz=args.serving_rate)
     cb = r["continuous_batching"]
     line = {"metric": "serving photons/s; p50/p99/p99.9 request latency", "value": cb["photons_per_s"],
             "unit": UNIT, "n_gpus": 1, "latency_ms": {k: cb[k] for k in ("p50_ms", "p99_ms", "p99.9_ms")},
@@ -188,6 +195,107 @@ def run_serving_workload(args):
                                    "budget at 32 B per expected hit"},
             "serving": r}
     print(json.dumps(line), flush=True)
+
+
+def surrogate_inference_rate(device, n=1_000_000, net=None, reps=10):
+    """Device queries/s of the surrogate network's tcgen05 inference kernel on
+    n queries per batch (features drawn over the trained range)."""
+    import torch
+    from photonprop_b200 import surrogate as sg
+    own = net is None
+    if own:
+        net = sg.MLP(device, seed=1)
+        net.set_normalization([1.2, 0.0, 5.5, 0.5], [0.5, 0.6, 0.9, 0.5], [0, 0, 0, 0, 0], [1, 1, 1, 1, 1])
+    rng = np.random.default_rng(0)
+    x = np.stack([rng.uniform(np.log10(2), np.log10(150), n), rng.uniform(-1, 1, n), rng.uniform(4, 7, n),
+                  rng.integers(0, 2, n)], axis=1).astype(np.float32)
+    dev = torch.device("cuda", device)
+    d_x = torch.from_numpy(x).to(dev)
+    d_o = torch.empty((5, n), dtype=torch.float32, device=dev)
+    s = torch.cuda.Stream(device=dev)
+    for _ in range(3):
+        net.forward(d_x, d_o, n, physical=True, stream=s)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        net.forward(d_x, d_o, n, physical=True, stream=s)
+    e1.record(s)
+    s.synchronize()
+    t = e0.elapsed_time(e1) / 1e3 / reps
+    flops = 2.0 * (4 * 128 + 2 * 128 * 128 + 128 * 5) * n
+    if own:
+        net.close()
+    return {"queries": n, "seconds_per_batch": t, "queries_per_s": n / t, "tflops": flops / t / 1e12}
+
+
+def run_surrogate_workload(args):
+    """--workload surrogate: MC training set (mixed-batch geometry, 1e6 photons
+    per pair), training by the library's kernels, held-out accuracy against MC,
+    query rate against the MC kernel."""
+    import torch
+    import photonprop_b200 as pp
+    from photonprop_b200 import surrogate as sg
+    torch.cuda.set_device(0)
+    medium = pp.make_seawater(35.0, 2.0)
+    spec = pp.CherenkovSpectrum((300.0, 800.0), 20, medium)
+    opts = pp.RunOptions(mode="physical", g=0.95, t_max=1000.0, hist_bins=1000)
+    out = {}
+    with pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=0) as prop:
+        t0 = time.perf_counter()
+        train = sg.mc_dataset(prop, sg.training_pairs(args.train_pairs, 1_000_000, seed=args.seed,
+                                                      distance_law=args.train_distance), opts,
+                              full_weight_hits=args.full_weight_hits)
+        test_pairs = sg.training_pairs(args.test_pairs, 1_000_000, seed=args.seed + 1)
+        test = sg.mc_dataset(prop, test_pairs, opts)
+        t_data = time.perf_counter() - t0
+        s = sg.Surrogate(prop, opts, seed=args.seed)
+        t0 = time.perf_counter()
+        losses = s.fit(train, epochs=args.epochs, batch=4096, lr=2e-3)
+        t_train = time.perf_counter() - t0
+        pred = s.predict_features(test.x, physical=True)
+        raw = s.predict_features(test.x, physical=False)
+        acc = {}
+        for cut in (100, 1000, 10000):
+            g = test.hits >= cut
+            if g.sum():
+                rel = np.abs(pred[g, 0] - test.mu[g]) / test.mu[g]
+                acc[f"hits>={cut}"] = {"pairs": int(g.sum()), "median_rel_err": float(np.median(rel)),
+                                       "frac_within_5pct": float(np.mean(rel < 0.05)),
+                                       "sum_ratio": float(pred[g, 0].sum() / test.mu[g].sum())}
+        r2 = {}
+        for j, name in enumerate(["ln_mu_over_N", "logit_w", "ln_a1", "ln_a2", "ln_theta"]):
+            m = test.mask[:, j] > 0
+            if m.sum() > 2:
+                r2[name] = float(1 - np.mean((raw[m, j] - test.y[m, j]) ** 2) / np.var(test.y[m, j]))
+        inf = surrogate_inference_rate(0, 1_000_000, net=s.net)
+        # MC rate on the same kind of query (1e6 photons per pair)
+        mc_pairs = np.ascontiguousarray(test_pairs[:4096])
+        dev = torch.device("cuda", 0)
+        d_pairs = torch.from_numpy(mc_pairs.view(np.uint8).copy()).to(dev)
+        d_cnt = torch.zeros(4, dtype=torch.int64, device=dev)
+        d_st = torch.zeros((len(mc_pairs), 8), dtype=torch.float64, device=dev)
+        d_hi = torch.zeros((len(mc_pairs), 1000), dtype=torch.float64, device=dev)
+        d_h = torch.zeros(64, dtype=torch.uint8, device=dev)
+        o = pp.RunOptions(**{**opts.__dict__})
+        o.write_hits = False
+        prop.propagate_device(d_pairs, len(mc_pairs), o, d_h, 0, d_cnt, d_st, d_hi)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        prop.propagate_device(d_pairs, len(mc_pairs), o, d_h, 0, d_cnt, d_st, d_hi)
+        e1.record()
+        torch.cuda.synchronize()
+        mc_rate = len(mc_pairs) / (e0.elapsed_time(e1) / 1e3)
+        out = {"metric": "surrogate queries/s and hit-count error vs MC", "value": inf["queries_per_s"],
+               "unit": "queries/s", "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+               "config": {"workload": f"{args.train_pairs} training ({args.train_distance} distance) + {args.test_pairs} "
+                                      "held-out pairs of the mixed-batch geometry, 1e6 photons each; MLP 4-128-128-128-5 GELU, "
+                                      f"BF16/FP32-acc, Adam 2e-3 cosine-decayed, batch 4096, {args.epochs} epochs; "
+                                      "inference at 1e6 queries per batch"},
+               "inference": inf, "mc_queries_per_s": mc_rate, "speedup_vs_mc": inf["queries_per_s"] / mc_rate,
+               "held_out_mu": acc, "held_out_r2": r2, "loss_first_last": [losses[0], losses[-1]],
+               "seconds": {"mc_dataset": t_data, "training": t_train}}
+    print(json.dumps(out), flush=True)
 
 
 def run_reference(args):
@@ -382,6 +490,8 @@ def run_ours(args):
         d2h += 32 + min(nh, cap) * 64 + n_pairs * 8 * 8 + n_pairs * bins * 8
     e2e_value = photons_all / reduce(e2e_t, MAX)
 
+    surrogate_inf = surrogate_inference_rate(local)
+
     serve = None
     if args.serving_seconds > 0:
         serve = run_serving(prop, args.serving_seconds, seed=args.seed + rank)
@@ -422,6 +532,7 @@ def run_ours(args):
                 "d2h_bytes_per_step": int(d2h / K)},
         "plain": plain,
         "serving": serve,
+        "surrogate_inference": surrogate_inf,
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
@@ -441,6 +552,13 @@ def main():
         run_reference(args)
     elif args.workload == "serving":
         run_serving_workload(args)
+    elif args.workload == "surrogate":
+        run_surrogate_workload(args)
+    elif args.workload == "surrogate-infer":
+        import torch
+        torch.cuda.set_device(0)
+        print(json.dumps({"metric": "surrogate inference queries/s (untrained weights)",
+                          **surrogate_inference_rate(0, 1_000_000)}), flush=True)
     else:
         run_ours(args)
 

@@ -48,12 +48,21 @@ struct Request {
 };
 using ReqPtr = std::shared_ptr<Request>;
 
+// Buffers grow by doubling (at least 1 MiB) so that reallocation, whose free
+// synchronises the device, stays rare in a running server.
+inline size_t grown(size_t have, size_t need) {
+  size_t n = std::max<size_t>(have, (size_t)1 << 20);
+  while (n < need) n *= 2;
+  return n;
+}
+
 struct DBuf {
   void* p = nullptr;
   size_t bytes = 0;
   cudaError_t ensure(size_t n) {
     if (n == 0) n = 16;
     if (bytes >= n) return cudaSuccess;
+    n = grown(bytes, n);
     if (p) cudaFree(p);
     p = nullptr;
     bytes = 0;
@@ -74,6 +83,7 @@ struct HBuf {
   cudaError_t ensure(size_t n) {
     if (n == 0) n = 16;
     if (bytes >= n) return cudaSuccess;
+    n = grown(bytes, n);
     if (p) cudaFreeHost(p);
     p = nullptr;
     bytes = 0;
@@ -334,6 +344,13 @@ pp_status pp_server_create(pp_ctx* ctx, const pp_server_config* cfg, pp_server**
       delete S;
       return PP_ERR_CUDA;
     }
+    // size for a full batch up front (pairs, scratch, statistics, histograms)
+    const size_t np = (size_t)c.max_pairs_per_batch, bins = (size_t)std::max(c.opts.hist_bins, 1);
+    if (s->d_pairs.ensure(np * sizeof(pp_pair)) || s->d_offsets.ensure((np + 1) * 8) || s->d_queue.ensure(64) ||
+        s->d_counters.ensure(64) || s->d_stats.ensure(np * PP_STATS * 8) || s->d_hist.ensure(np * bins * 8) ||
+        s->h_pairs.ensure(np * sizeof(pp_pair)) || s->h_counters.ensure(64) || s->h_stats.ensure(np * PP_STATS * 8) ||
+        s->h_hist.ensure(np * bins * 8) || s->d_hits.ensure((size_t)16 << 20) || s->h_hits.ensure((size_t)16 << 20))
+      cudaGetLastError();  // a failed pre-allocation is retried at launch
     S->slots.push_back(std::move(s));
   }
   cudaSetDevice(prev);

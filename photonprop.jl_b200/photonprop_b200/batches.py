@@ -55,7 +55,7 @@ def _unit_vectors(rng, n):
 
 
 def mixed_batch(n_pairs=4096, seed=0, n_min=1e4, n_max=1e7, d_min=2.0, d_max=150.0, radius=0.21,
-                track_len=1.0, cone_fraction=0.5):
+                track_len=1.0, cone_fraction=0.5, distance_law="uniform"):
     rng = np.random.Generator(np.random.PCG64(seed))
     out = np.zeros(n_pairs, dtype=_lib.PAIR_DTYPE)
     n = np.exp(rng.uniform(np.log(n_min), np.log(n_max), n_pairs))
@@ -64,7 +64,10 @@ def mixed_batch(n_pairs=4096, seed=0, n_min=1e4, n_max=1e7, d_min=2.0, d_max=150
     out["emitter"] = np.where(cone, _lib.EMITTER_CHERENKOV_CONE, _lib.EMITTER_ISOTROPIC)
     out["dir"] = _unit_vectors(rng, n_pairs)
     out["track_len"] = np.where(cone, track_len, 0.0)
-    dist = rng.uniform(d_min, d_max, n_pairs)
+    if distance_law == "loguniform":
+        dist = np.exp(rng.uniform(np.log(d_min), np.log(d_max), n_pairs))
+    else:
+        dist = rng.uniform(d_min, d_max, n_pairs)
     out["target"] = _unit_vectors(rng, n_pairs) * dist[:, None]
     out["radius"] = radius
     out["seed"] = [pair_seed(seed, i) for i in range(n_pairs)]

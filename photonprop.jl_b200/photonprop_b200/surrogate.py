@@ -137,7 +137,7 @@ class Dataset:
 
 
 def mc_dataset(prop: Propagator, pairs, opts: RunOptions, min_hits_mu=1, min_hits_fit=1000, chunk=20000,
-               fit_iters=60) -> Dataset:
+               fit_iters=60, full_weight_hits=100.0) -> Dataset:
     """Propagates the pairs (MC kernel, histograms only) and turns their
     statistics and histograms into targets."""
     import torch
@@ -173,8 +173,8 @@ def mc_dataset(prop: Propagator, pairs, opts: RunOptions, min_hits_mu=1, min_hit
         good_fit = (nh >= min_hits_fit) & np.all(np.isfinite(y[:, 1:]), axis=1)
         m = np.zeros_like(y)
         # loss weight of ln(mu/N): its Poisson variance is ~1/hits, so pairs with
-        # few hits count less (full weight from 100 hits)
-        m[:, 0] = np.where(nh >= max(min_hits_mu, 1), np.minimum(nh / 100.0, 1.0), 0.0)
+        # few hits count less (full weight from full_weight_hits hits)
+        m[:, 0] = np.where(nh >= max(min_hits_mu, 1), np.minimum(nh / full_weight_hits, 1.0), 0.0)
         m[:, 1] = good_fit
         m[:, 2] = good_fit & (w > 0.02)  # a component's shape is only measured if it carries weight
         m[:, 3] = good_fit & (w < 0.98)
@@ -189,9 +189,9 @@ def mc_dataset(prop: Propagator, pairs, opts: RunOptions, min_hits_mu=1, min_hit
     return Dataset(*(np.concatenate(cols[k]) for k in ("x", "y", "m", "h", "mu", "sg")))
 
 
-def training_pairs(n_pairs, photons, seed=0, d_min=2.0, d_max=150.0):
+def training_pairs(n_pairs, photons, seed=0, d_min=2.0, d_max=150.0, distance_law="uniform"):
     """The mixed-batch geometry with a fixed photon count per pair."""
-    b = mixed_batch(n_pairs, seed=seed, d_min=d_min, d_max=d_max)
+    b = mixed_batch(n_pairs, seed=seed, d_min=d_min, d_max=d_max, distance_law=distance_law)
     b["n_photons"] = int(photons)
     return b
 
@@ -206,7 +206,8 @@ class Surrogate:
         self.lo = None
         self.hi = None
 
-    def fit(self, data: Dataset, epochs=60, batch=4096, lr=1e-3, seed=0, log=None):
+    def fit(self, data: Dataset, epochs=60, batch=4096, lr=1e-3, seed=0, log=None, lr_min=1e-5):
+        """Adam with a cosine learning-rate decay from lr to lr_min."""
         import torch
         dev = torch.device("cuda", self.net.device)
         x, y, m = data.x, data.y, data.mask
@@ -228,12 +229,13 @@ class Surrogate:
         n = len(x)
         losses = []
         for ep in range(epochs):
+            lr_e = lr_min + 0.5 * (lr - lr_min) * (1.0 + np.cos(np.pi * ep / max(epochs, 1)))
             perm = torch.from_numpy(rng.permutation(n)).to(dev)
             tot, nb = 0.0, 0
             for s in range(0, n - batch + 1, batch):
                 idx = perm[s:s + batch]
                 loss, _ = self.net.train_step(xn[idx].contiguous(), yn[idx].contiguous(), mk[idx].contiguous(),
-                                              batch, lr)
+                                              batch, lr_e)
                 tot += loss
                 nb += 1
             losses.append(tot / max(nb, 1))
