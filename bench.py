@@ -57,7 +57,8 @@ def parse():
     ap.add_argument("--serving-seconds", type=float, default=10.0,
                     help="length of the serving sample in the default run (0 = skip)")
     ap.add_argument("--serving-rate", type=float, default=200.0, help="request arrival rate, Hz")
-    ap.add_argument("--workload", choices=["batch", "serving", "surrogate", "surrogate-infer"], default="batch")
+    ap.add_argument("--workload", choices=["batch", "serving", "surrogate", "surrogate-infer", "cone-grid", "point"],
+                    default="batch")
     ap.add_argument("--train-pairs", type=int, default=200_000)
     ap.add_argument("--test-pairs", type=int, default=20_000)
     ap.add_argument("--epochs", type=int, default=400)
@@ -296,6 +297,82 @@ def run_surrogate_workload(args):
                "held_out_mu": acc, "held_out_r2": r2, "loss_first_last": [losses[0], losses[-1]],
                "seconds": {"mc_dataset": t_data, "training": t_train}}
     print(json.dumps(out), flush=True)
+
+
+def run_cone_grid(args):
+    """--workload cone-grid: a 1 m Cherenkov track along +z, 1e8 photons per
+    launch, spheres at {5,10,20,50,100} m x polar {0,45,90,135,180} deg; PMT
+    weighting from the 5 nm table; one pair per launch (plain) and all 25 in
+    one batched launch."""
+    import torch
+    import photonprop_b200 as pp
+    torch.cuda.set_device(0)
+    medium = pp.make_seawater(35.0, 2.0)
+    spec = pp.CherenkovSpectrum((300.0, 800.0), 20, medium)
+    pairs = pp.batches.cone_grid_pairs(n_photons=100_000_000, seed=args.seed)
+    ro = pp.RunOptions(mode="physical", g=0.95, t_max=1000.0, hist_bins=1000)
+    with pp.Propagator(medium, spec, pp.p_one_pmt_acc_5nm, device=0) as prop:
+        prop.propagate_plain(pairs[:2], ro, hit_capacity=1 << 22)
+        t0 = time.perf_counter()
+        rp = prop.propagate_plain(pairs, ro, hit_capacity=1 << 24)
+        tp = time.perf_counter() - t0
+        prop.propagate(pairs, ro, hit_capacity=1 << 24)
+        t0 = time.perf_counter()
+        rb = prop.propagate(pairs, ro, hit_capacity=1 << 24)
+        tb = time.perf_counter() - t0
+    photons = float(pairs["n_photons"].sum())
+    line = {"metric": "propagated photons/s, one pair per launch (cone grid)", "value": photons / tp,
+            "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "data": "synthetic", "dtype": "f32",
+            "config": {"workload": "1 m Cherenkov track along +z, 1e8 photons per launch, r=0.21 m spheres at "
+                                   "{5,10,20,50,100} m x polar {0,45,90,135,180} deg (25 launches), PMT 5 nm table "
+                                   "300-700 nm (peak 0.2708), seawater 35 permille 2 degC, g=0.95"},
+            "plain_host_api_photons_per_s": photons / tp, "batched_host_api_photons_per_s": photons / tb,
+            "hits_per_pair": rp.stats[:, 0].tolist(), "sum_w_per_pair": rp.stats[:, 1].tolist(),
+            "identical_stats": bool(np.allclose(rp.stats, rb.stats, rtol=1e-9))}
+    print(json.dumps(line), flush=True)
+
+
+def run_point(args):
+    """--workload point: the small CPU-runnable case (isotropic point source,
+    1e5 photons, sphere at 10 m along +x, 500 x 1 ns histogram, seed 0) on the
+    GPU and through the FP64 oracle on all host cores, matched photon by photon."""
+    import torch
+    import photonprop_b200 as pp
+    from oracle import oracle as O
+    from oracle import tables as tb
+    torch.cuda.set_device(0)
+    medium = pp.make_seawater(35.0, 2.0)
+    spec = pp.CherenkovSpectrum((300.0, 800.0), 20, medium)
+    pair = pp.batches.point_source_pair(100_000, target=(10.0, 0.0, 0.0), seed=0)
+    ro = pp.RunOptions(mode="physical", g=0.95, t_max=500.0, hist_bins=500)
+    with pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=0) as prop:
+        for _ in range(3):
+            prop.propagate(pair, ro)
+        t0 = time.perf_counter()
+        r = prop.propagate(pair, ro)
+        tg = time.perf_counter() - t0
+        knots = prop.knots().astype(np.float64)
+    T = O.make_tables(tb.cascadia(35.0, 2.0), knots, pmt=(pp.p_one_pmt_acc.wavelengths, pp.p_one_pmt_acc.acceptance))
+    op = O.pairs_array(1)
+    for f in ("pos", "t0", "dir", "track_len", "target", "radius", "n_photons", "seed", "emitter"):
+        op[f] = pair[f]
+    c = ro.to_c()
+    oo = O.make_opts(mode=c.mode, max_steps=c.max_steps, g=float(np.float32(c.g)), t_max=c.t_max,
+                     hist_bins=c.hist_bins, flags=c.flags & 3)
+    t0 = time.perf_counter()
+    h, s, hist, steps, total = O.propagate(T, op, oo, n_threads=os.cpu_count() or 1)
+    tc = time.perf_counter() - t0
+    gk = {int(x["photon"]): x for x in r.hits}
+    ok = {int(x["photon"]): x for x in h}
+    both = sorted(set(gk) & set(ok))
+    dt = max((abs(float(gk[k]["time"]) - ok[k]["time"]) for k in both), default=0.0)
+    line = {"metric": "isotropic point source, 1e5 photons: hits, histogram, GPU vs FP64 oracle",
+            "value": 1e5 / tg, "unit": UNIT, "n_gpus": 1, "data": "synthetic",
+            "gpu_e2e_seconds": tg, "cpu_oracle_seconds": tc, "cpu_cores": os.cpu_count(),
+            "hits_gpu": r.n_hits, "hits_oracle": int(total), "matched": len(both), "max_abs_dt_ns": dt,
+            "sum_w_gpu": float(r.stats[0, 1]), "sum_w_oracle": float(s[0, 1]),
+            "hist_nonzero_bins": int(np.count_nonzero(r.hist[0]))}
+    print(json.dumps(line), flush=True)
 
 
 def run_reference(args):
@@ -554,6 +631,10 @@ def main():
         run_serving_workload(args)
     elif args.workload == "surrogate":
         run_surrogate_workload(args)
+    elif args.workload == "cone-grid":
+        run_cone_grid(args)
+    elif args.workload == "point":
+        run_point(args)
     elif args.workload == "surrogate-infer":
         import torch
         torch.cuda.set_device(0)
