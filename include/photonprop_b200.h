@@ -269,6 +269,72 @@ PP_API pp_status pp_cuda_propagate_photons(pp_ctx* ctx, float* d_out_positions,
                                     const pp_pair* source_target, const pp_run_opts* opts,
                                     void* stream);
 
+/* ---- fit stage: Cherenkov reweighting and Gamma fits -------------------- */
+/* The caller of the hot path in the reference (src/modelling.jl:46-111,
+ * src/emission.jl:32-99): photons propagated from an isotropic source are
+ * reweighted to the Cherenkov angular distribution of an EM cascade at each
+ * observation angle a,
+ *   w_dir = cherenkov_ang_dist(cos(theta0 - a), n) / (2 cherenkov_ang_dist_int(n)),
+ * (theta0 the emission polar angle, n the phase index at the photon's
+ * wavelength), multiplied by the hit weight, and a Gamma distribution is
+ * fitted by maximum likelihood to the weighted arrival-time residuals
+ * tres = t - (|target - source| - r) n(800 nm) / c with tres >= 0.  The
+ * detection fraction is the summed weight of all hits over the photons
+ * generated. */
+#define PP_FIT_MOMENTS 4 /* per (pair, angle): sum w (all hits), then over tres >= 0:
+                            sum w, sum w tres, sum w ln(tres) */
+#define PP_FIT_OUT 3     /* per (pair, angle): fit_alpha, fit_theta, det_fraction */
+#define PP_MAX_FIT_ANGLES 4096
+/* cherenkov_ang_dist with the e- parameters (4.27033, -6.02527, 0.29887,
+ * -0.00103), src/emission.jl:19-44. */
+PP_API double pp_cherenkov_ang_dist(double costheta, double ref_index);
+/* _cherenkov_ang_dist_int over [lower, upper], the reference's closed form
+ * with the upper incomplete gamma function, src/emission.jl:52-86. */
+PP_API double pp_cherenkov_ang_dist_int_exact(double ref_index, double lower, double upper);
+/* cherenkov_ang_dist_int: linear interpolation of the [-1, 1] integral on
+ * ref_index = 1.1:0.01:1.5, src/emission.jl:88-99 (NaN outside). */
+PP_API double pp_cherenkov_ang_dist_int(double ref_index);
+/* get_dir_reweight(thetas, obs_angle, ref_ixs), src/modelling.jl:46-49:
+ * out[i] = cherenkov_ang_dist(cos(thetas[i] - obs_angle), ref_ixs[i]) /
+ *          (2 cherenkov_ang_dist_int(ref_ixs[i])). */
+PP_API pp_status pp_dir_reweight(const double* thetas, double obs_angle, const double* ref_ixs, double* out,
+                                 int64_t n);
+
+/* Propagates the batch (as pp_propagate, full hit records kept on the
+ * device, hit_capacity of them) and runs the fit stage on the device for
+ * every pair and each of the n_angles observation angles (radians, host
+ * array): fits = n_pairs x n_angles x PP_FIT_OUT doubles (fit_alpha and
+ * fit_theta of the weighted Gamma maximum-likelihood fit, NaN where no hit
+ * has tres >= 0; det_fraction); moments (may be NULL) = n_pairs x n_angles x
+ * PP_FIT_MOMENTS; stats / hist as pp_propagate (may be NULL).  The whole of
+ * make_photon_fits (src/modelling.jl:86-111) for all distances is one call.
+ * PP_ERR_OVERFLOW when the hits exceed hit_capacity (the fits then cover
+ * only the stored hits; *n_hits holds the true count). */
+PP_API pp_status pp_propagate_fit(pp_ctx* ctx, const pp_pair* pairs, int64_t n_pairs,
+                                  const pp_run_opts* opts, const double* obs_angles, int32_t n_angles,
+                                  int64_t hit_capacity, int64_t* n_hits, double* fits, double* moments,
+                                  double* stats, double* hist);
+
+/* Device-buffer form of the fit stage over hits already on the device (full
+ * pp_hit records from pp_propagate_device with the same pairs and mode):
+ * hits counted by d_counters[0] (at most hit_capacity are read).  d_moments
+ * and d_fits as above, device memory; obs_angles is a host array. */
+PP_API pp_status pp_fit_hits_device(pp_ctx* ctx, const pp_pair* d_pairs, int64_t n_pairs, int32_t mode,
+                                    const pp_hit* d_hits, int64_t hit_capacity, const uint64_t* d_counters,
+                                    const double* obs_angles, int32_t n_angles, double* d_moments,
+                                    double* d_fits, void* stream);
+
+/* fit_photon_dist(obs_angles, obs_photon_df, n_ph_gen), src/modelling.jl:52-79,
+ * over a hit table given as FP64 device columns (tres, initial_theta,
+ * ref_ix, abs_weight, wavelength; n rows): the PMT acceptance of the
+ * context is applied to each photon's wavelength as the reference does.
+ * d_moments: n_angles x PP_FIT_MOMENTS, d_fits: n_angles x PP_FIT_OUT. */
+PP_API pp_status pp_fit_photon_dist_device(pp_ctx* ctx, int64_t n, const double* d_tres,
+                                           const double* d_initial_theta, const double* d_ref_ix,
+                                           const double* d_abs_weight, const double* d_wavelength,
+                                           const double* obs_angles, int32_t n_angles, int64_t n_ph_gen,
+                                           double* d_moments, double* d_fits, void* stream);
+
 /* ---- serving: continuous batching ----------------------------------------- */
 /* A request is a list of pairs.  A scheduler thread admits waiting requests
  * while their hit buffers fit the HBM budget (bytes_per_hit per expected hit)

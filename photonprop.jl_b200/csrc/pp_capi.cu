@@ -117,6 +117,9 @@ struct pp_ctx {
   uint64_t graph_clock = 0;
   pp_medium_desc medium;
   pp_pmt_desc pmt;
+  // fit stage: constants and device buffers
+  pp::FitConsts fitk;
+  DevBuf fit_counts, fit_rec, fit_moments, fit_out, fit_cs;
 
   pp_status fail(pp_status s, const std::string& msg) {
     err = msg;
@@ -414,6 +417,7 @@ pp_status pp_create(pp_ctx** out, int device, const pp_medium_desc* medium, cons
     pw[i] = (float)pmt->wavelength[i];
     pa[i] = (float)pmt->acceptance[i];
   }
+  pp::fill_fit_consts(&c->fitk, pp_refractive_index(medium, 800.0), pp_group_index(medium, 800.0));
   c->h_tables.resize(pp::dev_tables_size());
   pp::fill_dev_tables(c->h_tables.data(), coeffs, fk, n_knots, aw, al, n_abs, pw.data(), pa.data(), n_pmt);
   if ((e = cudaMalloc(&c->d_tables, c->h_tables.size())) ||
@@ -436,7 +440,9 @@ void pp_destroy(pp_ctx* c) {
     DeviceGuard guard(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->drop_graphs();
-    for (DevBuf* b : {&c->pairs, &c->hits, &c->counters, &c->stats, &c->hist, &c->offsets, &c->queue}) b->release();
+    for (DevBuf* b : {&c->pairs, &c->hits, &c->counters, &c->stats, &c->hist, &c->offsets, &c->queue, &c->fit_counts,
+                      &c->fit_rec, &c->fit_moments, &c->fit_out, &c->fit_cs})
+      b->release();
     if (c->d_tables) cudaFree(c->d_tables);
     if (c->stream) cudaStreamDestroy(c->stream);
   }
@@ -712,6 +718,150 @@ pp_status pp_device_eval(pp_ctx* c, int32_t op, const double* in, double* out, i
   cudaFree(din);
   cudaFree(dout);
   if (e) return c->cuda_fail(e, "pp_device_eval");
+  return PP_OK;
+}
+
+namespace {
+// Uploads cos/sin of the observation angles into the context's buffer.
+pp_status upload_angles(pp_ctx* c, const double* obs_angles, int32_t n_angles, cudaStream_t s) {
+  if (n_angles < 1 || n_angles > PP_MAX_FIT_ANGLES || !obs_angles)
+    return c->fail(PP_ERR_ARG, "need 1 <= n_angles <= PP_MAX_FIT_ANGLES observation angles");
+  std::vector<float2> cs(n_angles);
+  for (int i = 0; i < n_angles; ++i) {
+    if (!std::isfinite(obs_angles[i])) return c->fail(PP_ERR_ARG, "observation angles must be finite");
+    cs[i] = make_float2((float)std::cos(obs_angles[i]), (float)std::sin(obs_angles[i]));
+  }
+  bool grew = false;
+  cudaError_t e;
+  if ((e = ensure(c->fit_cs, cs.size() * sizeof(float2), &grew))) return alloc_fail(c, e, "fit angles");
+  if ((e = cudaMemcpyAsync(c->fit_cs.p, cs.data(), cs.size() * sizeof(float2), cudaMemcpyHostToDevice, s)))
+    return c->cuda_fail(e, "copy fit angles");
+  return PP_OK;
+}
+
+// Fit stage over hits on the device (the context's or the caller's).
+pp_status fit_hits(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs, int32_t mode, const pp_hit* d_hits,
+                   int64_t cap, const uint64_t* d_counters, const double* obs_angles, int32_t n_angles,
+                   double* d_moments, double* d_fits, cudaStream_t s) {
+  pp_status st = upload_angles(c, obs_angles, n_angles, s);
+  if (st) return st;
+  bool grew = false;
+  cudaError_t e;
+  if ((e = ensure(c->fit_counts, (size_t)std::max<int64_t>(n_pairs, 1) * sizeof(unsigned long long), &grew)) ||
+      (e = ensure(c->fit_rec, (size_t)std::max<int64_t>(cap, 1) * sizeof(pp::FitRec), &grew)))
+    return alloc_fail(c, e, "fit scratch");
+  if ((e = pp::launch_fit_hits(c->fitk, c->d_tables, d_pairs, n_pairs, mode, d_hits, (unsigned long long)cap,
+                               reinterpret_cast<const unsigned long long*>(d_counters),
+                               static_cast<unsigned long long*>(c->fit_counts.p),
+                               static_cast<pp::FitRec*>(c->fit_rec.p), static_cast<const float2*>(c->fit_cs.p),
+                               n_angles, d_moments, d_fits, c->sm_count, s)))
+    return c->cuda_fail(e, "fit stage");
+  return PP_OK;
+}
+}  // namespace
+
+pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp_run_opts* opts,
+                           const double* obs_angles, int32_t n_angles, int64_t cap, int64_t* n_hits, double* fits,
+                           double* moments, double* stats, double* hist) {
+  if (!c) return PP_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  pp_status st = validate_opts(c, opts);
+  if (st) return st;
+  if ((st = validate_pairs(c, pairs, n_pairs, opts->mode))) return st;
+  if (cap < 0 || !n_hits || !fits) return c->fail(PP_ERR_ARG, "pp_propagate_fit: bad buffer arguments");
+  if (n_angles < 1 || n_angles > PP_MAX_FIT_ANGLES || !obs_angles)
+    return c->fail(PP_ERR_ARG, "need 1 <= n_angles <= PP_MAX_FIT_ANGLES observation angles");
+  pp_run_opts o = *opts;
+  o.flags &= ~(uint32_t)(PP_OPT_NO_HITS | PP_OPT_COMPACT_HITS);  // the fit reads full hit records
+  if (!hist) o.hist_bins = 0;
+  const int bins = o.hist_bins;
+  DeviceGuard guard(c->device);
+  cudaError_t e;
+  bool grew = false;
+  if ((e = ensure(c->pairs, (size_t)n_pairs * sizeof(pp_pair), &grew)) ||
+      (e = ensure(c->hits, (size_t)cap * sizeof(pp_hit), &grew)) || (e = ensure(c->counters, 64, &grew)) ||
+      (e = ensure(c->stats, (size_t)n_pairs * PP_STATS * sizeof(double), &grew)) ||
+      (e = ensure(c->hist, (size_t)n_pairs * (size_t)(bins > 0 ? bins : 1) * sizeof(double), &grew)) ||
+      (e = ensure(c->offsets, (size_t)(n_pairs + 1) * sizeof(unsigned long long), &grew)) ||
+      (e = ensure(c->queue, 64, &grew)) ||
+      (e = ensure(c->fit_moments, (size_t)n_pairs * n_angles * PP_FIT_MOMENTS * sizeof(double) + 8, &grew)) ||
+      (e = ensure(c->fit_out, (size_t)n_pairs * n_angles * PP_FIT_OUT * sizeof(double) + 8, &grew)))
+    return alloc_fail(c, e, "pp_propagate_fit buffers");
+  if (grew) c->drop_graphs();
+  cudaStream_t s = c->stream;
+  if (n_pairs > 0 &&
+      (e = cudaMemcpyAsync(c->pairs.p, pairs, (size_t)n_pairs * sizeof(pp_pair), cudaMemcpyHostToDevice, s)))
+    return c->cuda_fail(e, "copy pairs");
+  pp::LaunchArgs a = base_args(c, &o);
+  a.pairs = static_cast<const pp_pair*>(c->pairs.p);
+  a.n_pairs = n_pairs;
+  a.chunk_offsets = static_cast<unsigned long long*>(c->offsets.p);
+  a.queue = static_cast<unsigned long long*>(c->queue.p);
+  a.hits = static_cast<pp_hit*>(c->hits.p);
+  a.hit_cap = (unsigned long long)cap;
+  a.counters = static_cast<unsigned long long*>(c->counters.p);
+  a.stats = static_cast<double*>(c->stats.p);
+  a.hist = bins > 0 ? static_cast<double*>(c->hist.p) : nullptr;
+  if ((e = run_batched(c, a, s, true))) return c->cuda_fail(e, "batched launch");
+  if ((st = fit_hits(c, a.pairs, n_pairs, o.mode, a.hits, cap, reinterpret_cast<const uint64_t*>(a.counters),
+                     obs_angles, n_angles, static_cast<double*>(c->fit_moments.p),
+                     static_cast<double*>(c->fit_out.p), s)))
+    return st;
+  unsigned long long cnt[4];
+  const size_t rows = (size_t)n_pairs * n_angles;
+  if ((e = cudaMemcpyAsync(cnt, c->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, s)) ||
+      (rows && (e = cudaMemcpyAsync(fits, c->fit_out.p, rows * PP_FIT_OUT * sizeof(double), cudaMemcpyDeviceToHost, s))) ||
+      (rows && moments &&
+       (e = cudaMemcpyAsync(moments, c->fit_moments.p, rows * PP_FIT_MOMENTS * sizeof(double), cudaMemcpyDeviceToHost, s))) ||
+      (n_pairs > 0 && stats &&
+       (e = cudaMemcpyAsync(stats, c->stats.p, (size_t)n_pairs * PP_STATS * sizeof(double), cudaMemcpyDeviceToHost, s))) ||
+      (n_pairs > 0 && bins > 0 &&
+       (e = cudaMemcpyAsync(hist, c->hist.p, (size_t)n_pairs * bins * sizeof(double), cudaMemcpyDeviceToHost, s))) ||
+      (e = cudaStreamSynchronize(s)))
+    return c->cuda_fail(e, "pp_propagate_fit copy back");
+  *n_hits = (int64_t)cnt[0];
+  if ((int64_t)cnt[0] > cap)
+    return c->fail(PP_ERR_OVERFLOW, "more hits than hit_capacity; the fits cover the stored hits only");
+  return PP_OK;
+}
+
+pp_status pp_fit_hits_device(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs, int32_t mode, const pp_hit* d_hits,
+                             int64_t cap, const uint64_t* d_counters, const double* obs_angles, int32_t n_angles,
+                             double* d_moments, double* d_fits, void* stream) {
+  if (!c) return PP_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (mode != PP_MODE_COMPAT && mode != PP_MODE_PHYSICAL) return c->fail(PP_ERR_ARG, "unknown mode");
+  if (n_pairs < 0 || n_pairs > (int64_t)INT32_MAX || (n_pairs > 0 && (!d_pairs || !d_moments || !d_fits)) ||
+      cap < 0 || (cap > 0 && !d_hits) || !d_counters)
+    return c->fail(PP_ERR_ARG, "pp_fit_hits_device: bad buffer arguments");
+  if (!aligned(d_pairs, 16) || !aligned(d_hits, 16) || !aligned(d_moments, 8) || !aligned(d_fits, 8))
+    return c->fail(PP_ERR_ARG, "pp_fit_hits_device: pairs/hits need 16-byte, moments/fits 8-byte alignment");
+  DeviceGuard guard(c->device);
+  return fit_hits(c, d_pairs, n_pairs, mode, d_hits, cap, d_counters, obs_angles, n_angles, d_moments, d_fits,
+                  static_cast<cudaStream_t>(stream));
+}
+
+pp_status pp_fit_photon_dist_device(pp_ctx* c, int64_t n, const double* d_tres, const double* d_theta,
+                                    const double* d_ref_ix, const double* d_abs_weight, const double* d_wavelength,
+                                    const double* obs_angles, int32_t n_angles, int64_t n_ph_gen, double* d_moments,
+                                    double* d_fits, void* stream) {
+  if (!c) return PP_ERR_ARG;
+  std::lock_guard<std::mutex> lk(c->mu);
+  if (n < 0 || (n > 0 && (!d_tres || !d_theta || !d_ref_ix || !d_abs_weight || !d_wavelength)) || !d_moments ||
+      !d_fits || n_ph_gen < 0)
+    return c->fail(PP_ERR_ARG, "pp_fit_photon_dist_device: bad arguments");
+  DeviceGuard guard(c->device);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  pp_status st = upload_angles(c, obs_angles, n_angles, s);
+  if (st) return st;
+  bool grew = false;
+  cudaError_t e;
+  if ((e = ensure(c->fit_rec, (size_t)std::max<int64_t>(n, 1) * sizeof(pp::FitRec), &grew)))
+    return alloc_fail(c, e, "fit scratch");
+  if ((e = pp::launch_fit_columns(c->fitk, c->d_tables, n, d_tres, d_theta, d_ref_ix, d_abs_weight, d_wavelength,
+                                  static_cast<pp::FitRec*>(c->fit_rec.p), static_cast<const float2*>(c->fit_cs.p),
+                                  n_angles, n_ph_gen, d_moments, d_fits, c->sm_count, s)))
+    return c->cuda_fail(e, "fit_photon_dist");
   return PP_OK;
 }
 

@@ -124,6 +124,87 @@ void default_abs_table(double* wl, double* len, int* n) {
 
 }  // namespace pp
 
+namespace pp {
+
+// Gamma(s, z), the upper incomplete gamma function, for s > 0, z >= 0.  Below
+// z = s + 1 it is Gamma(s) minus the lower function, whose power series
+// gamma(s, z) = z^s e^-z sum_k z^k / (s (s+1) ... (s+k)) converges fast there;
+// above, Legendre's continued fraction
+// Gamma(s, z) = e^-z z^s / (z + 1 - s - 1 (1 - s) / (z + 3 - s - 2 (2 - s) / ...))
+// evaluated by the modified Lentz method.
+double upper_incomplete_gamma(double s, double z) {
+  if (!(s > 0.0) || !(z >= 0.0)) return NAN;
+  if (z == 0.0) return std::tgamma(s);
+  const double lpre = s * std::log(z) - z;
+  if (z < s + 1.0) {
+    double term = 1.0 / s, sum = term;
+    for (int k = 1; k < 1000; ++k) {
+      term *= z / (s + k);
+      sum += term;
+      if (std::fabs(term) < std::fabs(sum) * 1e-17) break;
+    }
+    return std::tgamma(s) - std::exp(lpre) * sum;
+  }
+  const double tiny = 1e-300;
+  double b = z + 1.0 - s, c = 1.0 / tiny, d = 1.0 / b, f = d;
+  for (int k = 1; k < 1000; ++k) {
+    const double an = -k * (k - s);
+    b += 2.0;
+    d = an * d + b;
+    if (std::fabs(d) < tiny) d = tiny;
+    c = b + an / c;
+    if (std::fabs(c) < tiny) c = tiny;
+    d = 1.0 / d;
+    const double delta = d * c;
+    f *= delta;
+    if (std::fabs(delta - 1.0) < 1e-16) break;
+  }
+  return std::exp(lpre) * f;
+}
+
+// The reference's antiderivative of a exp(b |x - cos_c|^c) + d
+// (src/emission.jl:65-81): with u = |x - cos_c| and k = -b,
+// F(x) = d x + (a / c) (cos_c - x) Gamma(1/c, k u^c) (k u^c)^(-1/c); above the
+// peak the reference adds twice its value just below the peak
+// (peak_val = F(cos_c - 1e-5)), which is what joins the two branches in its
+// closed form.  Kept as the reference has it, including the d cos_c share of
+// peak_val, so that the normalisation matches.
+namespace {
+double ang_branch(double x, double cos_c, double u) {
+  const double k = -kAngB;
+  const double ku = k * std::pow(u, kAngC);
+  return (1.0 / kAngC) * (kAngC * kAngD * x +
+                          kAngA * (cos_c - x) * upper_incomplete_gamma(1.0 / kAngC, ku) * std::pow(ku, -1.0 / kAngC));
+}
+double ang_indef(double x, double cos_c) {
+  const double peak_val = ang_branch(cos_c - 1e-5, cos_c, 1e-5);
+  if (x <= cos_c) return ang_branch(x, cos_c, cos_c - x);
+  return ang_branch(x, cos_c, x - cos_c) + 2.0 * peak_val;
+}
+}  // namespace
+
+double cherenkov_ang_dist_int_closed(double ref_index, double lower, double upper) {
+  const double cos_c = 1.0 / ref_index;
+  return ang_indef(upper, cos_c) - ang_indef(lower, cos_c);
+}
+
+void cherenkov_ang_dist_int_table(double* out) {
+  for (int i = 0; i < kAngIntN; ++i) out[i] = cherenkov_ang_dist_int_closed(kAngIntN0 + kAngIntDn * i, -1.0, 1.0);
+}
+
+// LinearInterpolation(1.1:0.01:1.5, table) inside the range, NaN outside
+// (the reference's interpolation throws there).
+double ang_int_interp(const double* table, double n) {
+  const double x = (n - kAngIntN0) / kAngIntDn;
+  if (!(x >= -1e-9) || !(x <= kAngIntN - 1 + 1e-9)) return NAN;
+  int i = (int)std::floor(x);
+  i = std::min(std::max(i, 0), kAngIntN - 2);
+  const double f = x - i;
+  return table[i] + f * (table[i + 1] - table[i]);
+}
+
+}  // namespace pp
+
 extern "C" {
 
 double pp_refractive_index(const pp_medium_desc* m, double wl) {
@@ -188,6 +269,33 @@ pp_status pp_cherenkov_knots(const pp_medium_desc* m, double wl_min, double wl_m
     const double f = (u - cdf[k - 1]) / (cdf[k] - cdf[k - 1]);
     out[j] = wl[k - 1] + f * (wl[k] - wl[k - 1]);
   }
+  return PP_OK;
+}
+
+// ---- Cherenkov angular distribution of EM cascades (src/emission.jl:19-99) ----
+
+double pp_cherenkov_ang_dist(double costheta, double ref_index) {
+  const double cos_c = 1.0 / ref_index;
+  return pp::kAngA * std::exp(pp::kAngB * std::pow(std::fabs(costheta - cos_c), pp::kAngC)) + pp::kAngD;
+}
+
+double pp_cherenkov_ang_dist_int_exact(double ref_index, double lower, double upper) {
+  return pp::cherenkov_ang_dist_int_closed(ref_index, lower, upper);
+}
+
+double pp_cherenkov_ang_dist_int(double ref_index) {
+  double table[pp::kAngIntN];
+  pp::cherenkov_ang_dist_int_table(table);
+  return pp::ang_int_interp(table, ref_index);
+}
+
+pp_status pp_dir_reweight(const double* thetas, double obs_angle, const double* ref_ixs, double* out, int64_t n) {
+  if (n < 0 || (n > 0 && (!thetas || !ref_ixs || !out))) return PP_ERR_ARG;
+  double table[pp::kAngIntN];
+  pp::cherenkov_ang_dist_int_table(table);
+  for (int64_t i = 0; i < n; ++i)
+    out[i] = pp_cherenkov_ang_dist(std::cos(thetas[i] - obs_angle), ref_ixs[i]) /
+             (2.0 * pp::ang_int_interp(table, ref_ixs[i]));
   return PP_OK;
 }
 

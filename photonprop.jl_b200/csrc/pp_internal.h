@@ -60,6 +60,41 @@ pp_status propagate_with_scratch(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pa
 int ctx_device(const pp_ctx* c);
 int ctx_sm_count(const pp_ctx* c);
 
+// Cherenkov angular distribution of EM cascades, e- parameters
+// (src/emission.jl:19), and the reference's table of its [-1, 1] integral
+// over the refractive index 1.1:0.01:1.5 (src/emission.jl:88-99).
+constexpr double kAngA = 4.27033, kAngB = -6.02527, kAngC = 0.29887, kAngD = -0.00103;
+constexpr int kAngIntN = 41;
+constexpr double kAngIntN0 = 1.1, kAngIntDn = 0.01;
+double upper_incomplete_gamma(double s, double z);
+double cherenkov_ang_dist_int_closed(double ref_index, double lower, double upper);
+void cherenkov_ang_dist_int_table(double* out);
+double ang_int_interp(const double* table, double n);
+
+// fit stage (pp_fit.cu)
+struct FitConsts {
+  float a, b_l2, c, d;         // cherenkov_ang_dist parameters, b in base 2
+  float n800_phase, n800_group;  // refractive indices at 800 nm (tgeo)
+  float inv_dn;
+  float normf[kAngIntN];       // [-1, 1] integral on 1.1:0.01:1.5
+};
+struct FitRec {  // 32 bytes, one per hit
+  float ct, st, c0, wn;  // cos / sin of the emission polar angle, 1/n, weight / (2 int(n))
+  float tres, lnt;       // arrival-time residual and its log
+  int32_t pair;
+  int32_t pos;  // tres >= 0
+};
+static_assert(sizeof(FitRec) == 32, "FitRec is moved as two 16-byte words");
+void fill_fit_consts(FitConsts* K, double n800_phase, double n800_group);
+cudaError_t launch_fit_hits(const FitConsts& K, const void* tables, const pp_pair* pairs, int64_t n_pairs, int mode,
+                            const pp_hit* hits, unsigned long long cap, const unsigned long long* counters,
+                            unsigned long long* counts, FitRec* rec, const float2* cs, int n_angles,
+                            double* moments, double* fits, int sm_count, cudaStream_t s);
+cudaError_t launch_fit_columns(const FitConsts& K, const void* tables, int64_t n, const double* tres,
+                               const double* theta, const double* ref_ix, const double* abs_w, const double* wl,
+                               FitRec* rec, const float2* cs, int n_angles, int64_t n_gen, double* moments,
+                               double* fits, int sm_count, cudaStream_t s);
+
 // host physics (pp_host_physics.cpp)
 void medium_coeffs(const pp_medium_desc* m, double out[11]);
 void default_abs_table(double* wl, double* len, int* n);

@@ -33,6 +33,7 @@
 #include <vector>
 
 #include "pp_internal.h"
+#include "pp_special.cuh"
 
 namespace mlp {
 
@@ -612,24 +613,9 @@ __global__ void __launch_bounds__(THREADS, 1) gemm_test_kernel(const __nv_bfloat
 // SL_k / S0_k - ln theta solved by Newton (psi and psi' from their asymptotic
 // series after upward recurrence).  Output per pair: w, a1 <= a2, theta,
 // mean log-likelihood per weight; NaNs when the histogram is empty.
-__device__ double digamma_d(double x) {
-  double r = 0.0;
-  while (x < 6.0) {
-    r -= 1.0 / x;
-    x += 1.0;
-  }
-  const double f = 1.0 / (x * x);
-  return r + log(x) - 0.5 / x - f * (1.0 / 12 - f * (1.0 / 120 - f * (1.0 / 252 - f * (1.0 / 240 - f / 132))));
-}
-__device__ double trigamma_d(double x) {
-  double r = 0.0;
-  while (x < 6.0) {
-    r += 1.0 / (x * x);
-    x += 1.0;
-  }
-  const double f = 1.0 / (x * x);
-  return r + 1.0 / x + 0.5 * f + (1.0 / x) * f * (1.0 / 6 - f * (1.0 / 30 - f * (1.0 / 42 - f / 30)));
-}
+using ppsf::digamma_d;
+using ppsf::trigamma_d;
+
 // a with psi(a) = y (Minka's initialisation, Newton steps).
 __device__ double inv_digamma(double y) {
   double a = y >= -2.22 ? exp(y) + 0.5 : -1.0 / (y + 0.5772156649015329);

@@ -19,6 +19,7 @@ from . import batches
 from . import serving
 from . import parallel
 from . import surrogate
+from . import modelling
 
 
 def build(force=False):

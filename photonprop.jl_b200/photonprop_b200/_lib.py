@@ -124,6 +124,15 @@ _SIGS = [
                                                  _I64, _VP, _VP, _VP, _VP]),
     ("pp_cuda_propagate_photons", ctypes.c_int, [_VP, _VP, _VP, _VP, _VP, _VP, _VP, _I32, _I32, _I32,
                                                  _VP, ctypes.POINTER(RunOpts), _VP]),
+    ("pp_cherenkov_ang_dist", _D, [_D, _D]),
+    ("pp_cherenkov_ang_dist_int_exact", _D, [_D, _D, _D]),
+    ("pp_cherenkov_ang_dist_int", _D, [_D]),
+    ("pp_dir_reweight", ctypes.c_int, [_VP, _D, _VP, _VP, _I64]),
+    ("pp_propagate_fit", ctypes.c_int, [_VP, _VP, _I64, ctypes.POINTER(RunOpts), _VP, _I32, _I64,
+                                        ctypes.POINTER(_I64), _VP, _VP, _VP, _VP]),
+    ("pp_fit_hits_device", ctypes.c_int, [_VP, _VP, _I64, _I32, _VP, _I64, _VP, _VP, _I32, _VP, _VP, _VP]),
+    ("pp_fit_photon_dist_device", ctypes.c_int, [_VP, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _I32, _I64, _VP, _VP,
+                                                 _VP]),
     ("pp_server_create", ctypes.c_int, [_VP, ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
     ("pp_server_destroy", None, [_VP]),
     ("pp_server_submit", ctypes.c_int, [_VP, _VP, _I32, ctypes.POINTER(ctypes.c_uint64)]),
@@ -152,6 +161,10 @@ _SIGS = [
 ]
 
 EXPORTED = [s[0] for s in _SIGS]
+
+FIT_MOMENTS = 4
+FIT_OUT = 3
+MAX_FIT_ANGLES = 4096
 
 
 def load():
