@@ -57,8 +57,11 @@ def parse():
     ap.add_argument("--serving-seconds", type=float, default=10.0,
                     help="length of the serving sample in the default run (0 = skip)")
     ap.add_argument("--serving-rate", type=float, default=200.0, help="request arrival rate, Hz")
-    ap.add_argument("--workload", choices=["batch", "serving", "surrogate", "surrogate-infer", "cone-grid", "point"],
-                    default="batch")
+    ap.add_argument("--workload", choices=["batch", "serving", "surrogate", "surrogate-infer", "cone-grid", "point",
+                                           "fits"], default="batch")
+    ap.add_argument("--fit-photons", type=int, default=100_000_000, help="fits workload: photons per distance")
+    ap.add_argument("--fit-distances", type=int, default=250)
+    ap.add_argument("--fit-angles", type=int, default=250)
     ap.add_argument("--train-pairs", type=int, default=200_000)
     ap.add_argument("--test-pairs", type=int, default=20_000)
     ap.add_argument("--epochs", type=int, default=400)
@@ -375,6 +378,117 @@ def run_point(args):
     print(json.dumps(line), flush=True)
 
 
+def run_fits(args):
+    """--workload fits: make_photon_fits(1e8 photons, 250 distances, 250
+    angles, 300 m) as example_full.jl:136 calls it: compat mode, Cascadia
+    medium, PMT weight.  e2e = the public call (pairs built on the host, one
+    batched launch, reweighting and Gamma fits on the device, the fit table
+    back on the host).  The device breakdown times the propagation and the
+    fit stage with CUDA events; the CPU baseline is the FP64 oracle's
+    propagation of the first L photons of every distance plus its fits."""
+    import torch
+    import photonprop_b200 as pp
+    from photonprop_b200 import modelling as md
+    torch.cuda.set_device(0)
+    n_ph, n_d, n_a, maxd = args.fit_photons, args.fit_distances, args.fit_angles, 300.0
+    m = pp.make_cascadia_medium_properties()
+    spec = pp.CherenkovSpectrum((300.0, 800.0), 20, m)
+    ro = pp.RunOptions(mode="compat", pmt_weight=True, hist_bins=0)
+    pairs, distances, angles = md.fit_pairs(n_ph, n_d, n_a, maxd, seed=args.seed)
+    with pp.Propagator(m, spec, pp.p_one_pmt_acc, device=0) as prop:
+        warm = md.propagate_fit(prop, pairs, angles, ro)  # allocates the buffers
+        cap = int(warm.n_hits * 1.05) + 4096  # the device breakdown keeps every hit
+        e2e = []
+        for _ in range(2):
+            t0 = time.perf_counter()
+            df = md.make_photon_fits(n_ph, n_d, n_a, maxd, propagator=prop, seed=args.seed)
+            e2e.append(time.perf_counter() - t0)
+        # device breakdown
+        dev = torch.device("cuda", 0)
+        d_pairs = torch.from_numpy(pairs.view(np.uint8).copy()).to(dev)
+        d_hits = torch.empty(cap * 64, dtype=torch.uint8, device=dev)
+        d_cnt = torch.zeros(4, dtype=torch.int64, device=dev)
+        d_stats = torch.zeros((n_d, 8), dtype=torch.float64, device=dev)
+        d_m = torch.zeros((n_d, n_a, 4), dtype=torch.float64, device=dev)
+        d_f = torch.zeros((n_d, n_a, 3), dtype=torch.float64, device=dev)
+        L = pp._lib.load()
+        stream = torch.cuda.current_stream(dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        t_prop, t_fit = [], []
+        for _ in range(4):
+            ev[0].record(stream)
+            prop.propagate_device(d_pairs, n_d, ro, d_hits, cap, d_cnt, d_stats, None, stream=stream)
+            ev[1].record(stream)
+            pp._lib.check(L.pp_fit_hits_device(prop.handle, d_pairs.data_ptr(), n_d, pp._lib.MODE_COMPAT,
+                                               d_hits.data_ptr(), cap, d_cnt.data_ptr(), angles.ctypes.data, n_a,
+                                               d_m.data_ptr(), d_f.data_ptr(), stream.cuda_stream), prop.handle)
+            ev[2].record(stream)
+            torch.cuda.synchronize()
+            t_prop.append(ev[0].elapsed_time(ev[1]) / 1e3)
+            t_fit.append(ev[1].elapsed_time(ev[2]) / 1e3)
+        hits = int(d_cnt[0].item())
+        knots = prop.knots().astype(np.float64)
+    photons = float(n_ph) * n_d
+    tp, tf = float(np.median(t_prop[1:])), float(np.median(t_fit[1:]))
+    line = {"metric": "make_photon_fits photons/s (propagation + reweighting + Gamma fits)",
+            "value": photons / min(e2e), "unit": UNIT, "n_gpus": 1, "higher_is_better": True, "data": "synthetic",
+            "dtype": "f32 (FP64 moments and fits)",
+            "config": {"workload": f"make_photon_fits({n_ph:.0e}, {n_d}, {n_a}, {maxd:.0f} m): isotropic source, "
+                                   "0.21 m sphere at Sobol distances, Sobol observation angles, compat mode, "
+                                   "Cascadia medium, PMT weight"},
+            "e2e_seconds": min(e2e), "hits": hits,
+            "device": {"propagation_s": tp, "fit_stage_s": tf, "propagation_photons_per_s": photons / tp,
+                       "fit_hit_angle_evals_per_s": hits * n_a / tf},
+            "fit_table_rows": len(df), "finite_fits": int(np.isfinite(df["fit_alpha"]).sum())}
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = fits_cpu_baseline(pairs, angles, knots, args.cpu_seconds)
+    print(json.dumps(line), flush=True)
+
+
+def fits_cpu_baseline(pairs, angles, knots, target_seconds):
+    """FP64 oracle: propagation of the first L photons of every distance
+    (all host threads) and the reweighting + Gamma fits of its hits."""
+    from oracle import fits as F
+    from oracle import oracle as O
+    from oracle import tables as tb
+    import photonprop_b200 as pp
+    m = tb.cascadia()
+    T = O.make_tables(m, knots, pmt=(pp.p_one_pmt_acc.wavelengths, pp.p_one_pmt_acc.acceptance))
+    op = O.pairs_array(len(pairs))
+    for f in ("pos", "t0", "dir", "track_len", "target", "radius", "n_photons", "seed", "emitter"):
+        op[f] = pairs[f]
+    oo = O.make_opts(mode=O.MODE_COMPAT, g=0.99, hist_bins=0, flags=O.OPT_PMT_WEIGHT)
+    cores = os.cpu_count() or 1
+
+    def run(lim):
+        t0 = time.perf_counter()
+        h, s, _, _, total = O.propagate(T, op, oo, photon_limit=lim, n_threads=cores, hit_cap=1 << 22)
+        n800 = tb.refractive_index(800.0, m)
+        tab = F.int_table()
+        for p in range(len(pairs)):
+            hp = h[h["pair"] == p]
+            if len(hp) == 0:
+                continue
+            d = float(np.linalg.norm(pairs["target"][p].astype(np.float64)))
+            tres = hp["time"] - (d - 0.21) * n800 / 0.299792458
+            theta = np.arccos(np.clip(hp["dir0"][:, 2], -1, 1))
+            n = tb.refractive_index(hp["wavelength"], m)
+            for a in angles:
+                mo = F.moments(tres, F.get_dir_reweight(theta, a, n, tab) * hp["weight"])
+                F.gamma_fit_moments(mo[1], mo[2], mo[3])
+        return time.perf_counter() - t0
+
+    lim = 2000
+    dt = max(run(lim), 1e-3)
+    lim = int(max(2000, min(int(pairs["n_photons"][0]), lim * target_seconds / dt)))
+    dt = run(lim)
+    photons = lim * len(pairs)
+    return {"value": photons / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"first {lim} photons of each of the {len(pairs)} distances ({photons:.3e} photons, {dt:.1f} s), "
+                      f"FP64 oracle propagation (OpenMP {cores} threads) + numpy reweighting/fits over "
+                      f"{len(angles)} angles"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -635,6 +749,8 @@ def main():
         run_cone_grid(args)
     elif args.workload == "point":
         run_point(args)
+    elif args.workload == "fits":
+        run_fits(args)
     elif args.workload == "surrogate-infer":
         import torch
         torch.cuda.set_device(0)

@@ -300,16 +300,17 @@ PP_API double pp_cherenkov_ang_dist_int(double ref_index);
 PP_API pp_status pp_dir_reweight(const double* thetas, double obs_angle, const double* ref_ixs, double* out,
                                  int64_t n);
 
-/* Propagates the batch (as pp_propagate, full hit records kept on the
- * device, hit_capacity of them) and runs the fit stage on the device for
- * every pair and each of the n_angles observation angles (radians, host
- * array): fits = n_pairs x n_angles x PP_FIT_OUT doubles (fit_alpha and
- * fit_theta of the weighted Gamma maximum-likelihood fit, NaN where no hit
- * has tres >= 0; det_fraction); moments (may be NULL) = n_pairs x n_angles x
- * PP_FIT_MOMENTS; stats / hist as pp_propagate (may be NULL).  The whole of
- * make_photon_fits (src/modelling.jl:86-111) for all distances is one call.
- * PP_ERR_OVERFLOW when the hits exceed hit_capacity (the fits then cover
- * only the stored hits; *n_hits holds the true count). */
+/* Propagates the batch (as pp_propagate) and runs the fit stage on the
+ * device for every pair and each of the n_angles observation angles
+ * (radians, host array): fits = n_pairs x n_angles x PP_FIT_OUT doubles
+ * (fit_alpha and fit_theta of the weighted Gamma maximum-likelihood fit, NaN
+ * where no hit has tres >= 0; det_fraction); moments (may be NULL) =
+ * n_pairs x n_angles x PP_FIT_MOMENTS; stats / hist as pp_propagate (may be
+ * NULL); *n_hits = all hits.  hit_capacity sizes the device hit buffer:
+ * pairs run in waves whose hits fit it (a wave that overflows is halved and
+ * run again), so it bounds memory, not the number of hits; PP_ERR_OVERFLOW
+ * only when one pair alone has more hits.  The whole of make_photon_fits
+ * (src/modelling.jl:86-111) for all distances is one call. */
 PP_API pp_status pp_propagate_fit(pp_ctx* ctx, const pp_pair* pairs, int64_t n_pairs,
                                   const pp_run_opts* opts, const double* obs_angles, int32_t n_angles,
                                   int64_t hit_capacity, int64_t* n_hits, double* fits, double* moments,

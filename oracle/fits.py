@@ -89,15 +89,23 @@ def gamma_fit_moments(sw, swx, swlx, tol=1e-14, maxiter=100):
     if not (s > 0 and np.isfinite(s)):
         return np.nan, np.nan
     a = (3.0 - s + np.sqrt((s - 3.0) ** 2 + 24.0 * s)) / (12.0 * s)
+    with np.errstate(all="ignore"):
+        a = _newton(a, ml, lmx, tol, maxiter)
+    if not (a > 0 and np.isfinite(a)):
+        return np.nan, np.nan
+    return a, mx / a
+
+
+def _newton(a, ml, lmx, tol, maxiter):
     for _ in range(maxiter):
         ia = 1.0 / a
         z = ia + (ml - lmx + np.log(a) - special.digamma(a)) / (a * a * (ia - special.polygamma(1, a)))
         an = 1.0 / z
         done = abs(an - a) <= tol * a
         a = an
-        if done:
+        if done or not a > 0:
             break
-    return a, mx / a
+    return a
 
 
 def gamma_fit(x, w):

@@ -739,7 +739,7 @@ pp_status upload_angles(pp_ctx* c, const double* obs_angles, int32_t n_angles, c
   return PP_OK;
 }
 
-// Fit stage over hits on the device (the context's or the caller's).
+// Fit stage over hits on the device (the caller's): moments, then fits.
 pp_status fit_hits(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs, int32_t mode, const pp_hit* d_hits,
                    int64_t cap, const uint64_t* d_counters, const double* obs_angles, int32_t n_angles,
                    double* d_moments, double* d_fits, cudaStream_t s) {
@@ -750,15 +750,29 @@ pp_status fit_hits(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs, int32_t m
   if ((e = ensure(c->fit_counts, (size_t)std::max<int64_t>(n_pairs, 1) * sizeof(unsigned long long), &grew)) ||
       (e = ensure(c->fit_rec, (size_t)std::max<int64_t>(cap, 1) * sizeof(pp::FitRec), &grew)))
     return alloc_fail(c, e, "fit scratch");
-  if ((e = pp::launch_fit_hits(c->fitk, c->d_tables, d_pairs, n_pairs, mode, d_hits, (unsigned long long)cap,
-                               reinterpret_cast<const unsigned long long*>(d_counters),
-                               static_cast<unsigned long long*>(c->fit_counts.p),
-                               static_cast<pp::FitRec*>(c->fit_rec.p), static_cast<const float2*>(c->fit_cs.p),
-                               n_angles, d_moments, d_fits, c->sm_count, s)))
+  if (n_pairs == 0) return PP_OK;
+  if ((e = cudaMemsetAsync(d_moments, 0, (size_t)n_pairs * n_angles * PP_FIT_MOMENTS * sizeof(double), s)) ||
+      (e = pp::launch_fit_moments_hits(c->fitk, c->d_tables, d_pairs, n_pairs, mode, d_hits, (unsigned long long)cap,
+                                       reinterpret_cast<const unsigned long long*>(d_counters),
+                                       static_cast<unsigned long long*>(c->fit_counts.p),
+                                       static_cast<pp::FitRec*>(c->fit_rec.p),
+                                       static_cast<const float2*>(c->fit_cs.p), n_angles, d_moments, c->sm_count,
+                                       s)) ||
+      (e = pp::launch_fit_gamma(d_moments, n_pairs, n_angles, d_pairs, 0, d_fits, s)))
     return c->cuda_fail(e, "fit stage");
   return PP_OK;
 }
 }  // namespace
+
+// Expected hits of a pair from geometry alone: the sphere's solid-angle
+// fraction r^2 / (4 d^2) of the photons (all of them from inside the sphere).
+static double expected_hits_geo(const pp_pair& q) {
+  const double dx = (double)q.target[0] - q.pos[0], dy = (double)q.target[1] - q.pos[1],
+               dz = (double)q.target[2] - q.pos[2];
+  const double d = std::sqrt(dx * dx + dy * dy + dz * dz), r = q.radius;
+  const double f = d <= r ? 1.0 : std::min(1.0, std::max(r * r / (4.0 * (d - r) * (d - r)), 1e-7));
+  return f * (double)q.n_photons;
+}
 
 pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp_run_opts* opts,
                            const double* obs_angles, int32_t n_angles, int64_t cap, int64_t* n_hits, double* fits,
@@ -768,7 +782,7 @@ pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, con
   pp_status st = validate_opts(c, opts);
   if (st) return st;
   if ((st = validate_pairs(c, pairs, n_pairs, opts->mode))) return st;
-  if (cap < 0 || !n_hits || !fits) return c->fail(PP_ERR_ARG, "pp_propagate_fit: bad buffer arguments");
+  if (cap < 1 || !n_hits || !fits) return c->fail(PP_ERR_ARG, "pp_propagate_fit: bad buffer arguments");
   if (n_angles < 1 || n_angles > PP_MAX_FIT_ANGLES || !obs_angles)
     return c->fail(PP_ERR_ARG, "need 1 <= n_angles <= PP_MAX_FIT_ANGLES observation angles");
   pp_run_opts o = *opts;
@@ -778,50 +792,87 @@ pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, con
   DeviceGuard guard(c->device);
   cudaError_t e;
   bool grew = false;
+  const size_t rows = (size_t)n_pairs * n_angles;
   if ((e = ensure(c->pairs, (size_t)n_pairs * sizeof(pp_pair), &grew)) ||
       (e = ensure(c->hits, (size_t)cap * sizeof(pp_hit), &grew)) || (e = ensure(c->counters, 64, &grew)) ||
       (e = ensure(c->stats, (size_t)n_pairs * PP_STATS * sizeof(double), &grew)) ||
       (e = ensure(c->hist, (size_t)n_pairs * (size_t)(bins > 0 ? bins : 1) * sizeof(double), &grew)) ||
       (e = ensure(c->offsets, (size_t)(n_pairs + 1) * sizeof(unsigned long long), &grew)) ||
       (e = ensure(c->queue, 64, &grew)) ||
-      (e = ensure(c->fit_moments, (size_t)n_pairs * n_angles * PP_FIT_MOMENTS * sizeof(double) + 8, &grew)) ||
-      (e = ensure(c->fit_out, (size_t)n_pairs * n_angles * PP_FIT_OUT * sizeof(double) + 8, &grew)))
+      (e = ensure(c->fit_moments, rows * PP_FIT_MOMENTS * sizeof(double) + 8, &grew)) ||
+      (e = ensure(c->fit_out, rows * PP_FIT_OUT * sizeof(double) + 8, &grew)) ||
+      (e = ensure(c->fit_counts, (size_t)std::max<int64_t>(n_pairs, 1) * sizeof(unsigned long long), &grew)) ||
+      (e = ensure(c->fit_rec, (size_t)cap * sizeof(pp::FitRec), &grew)))
     return alloc_fail(c, e, "pp_propagate_fit buffers");
   if (grew) c->drop_graphs();
   cudaStream_t s = c->stream;
+  if ((st = upload_angles(c, obs_angles, n_angles, s))) return st;
+  const pp_pair* d_pairs = static_cast<const pp_pair*>(c->pairs.p);
+  double* d_mom = static_cast<double*>(c->fit_moments.p);
   if (n_pairs > 0 &&
-      (e = cudaMemcpyAsync(c->pairs.p, pairs, (size_t)n_pairs * sizeof(pp_pair), cudaMemcpyHostToDevice, s)))
-    return c->cuda_fail(e, "copy pairs");
-  pp::LaunchArgs a = base_args(c, &o);
-  a.pairs = static_cast<const pp_pair*>(c->pairs.p);
-  a.n_pairs = n_pairs;
-  a.chunk_offsets = static_cast<unsigned long long*>(c->offsets.p);
-  a.queue = static_cast<unsigned long long*>(c->queue.p);
-  a.hits = static_cast<pp_hit*>(c->hits.p);
-  a.hit_cap = (unsigned long long)cap;
-  a.counters = static_cast<unsigned long long*>(c->counters.p);
-  a.stats = static_cast<double*>(c->stats.p);
-  a.hist = bins > 0 ? static_cast<double*>(c->hist.p) : nullptr;
-  if ((e = run_batched(c, a, s, true))) return c->cuda_fail(e, "batched launch");
-  if ((st = fit_hits(c, a.pairs, n_pairs, o.mode, a.hits, cap, reinterpret_cast<const uint64_t*>(a.counters),
-                     obs_angles, n_angles, static_cast<double*>(c->fit_moments.p),
-                     static_cast<double*>(c->fit_out.p), s)))
-    return st;
-  unsigned long long cnt[4];
-  const size_t rows = (size_t)n_pairs * n_angles;
-  if ((e = cudaMemcpyAsync(cnt, c->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, s)) ||
+      ((e = cudaMemcpyAsync(c->pairs.p, pairs, (size_t)n_pairs * sizeof(pp_pair), cudaMemcpyHostToDevice, s)) ||
+       (e = cudaMemsetAsync(d_mom, 0, rows * PP_FIT_MOMENTS * sizeof(double), s))))
+    return c->cuda_fail(e, "pp_propagate_fit setup");
+  // Waves of pairs whose hits fit the hit buffer: each wave propagates, then
+  // adds its hits' moments; the expected hits per pair are geometric, scaled
+  // by what the waves so far produced, and a wave that overflows is halved.
+  std::vector<double> est(n_pairs);
+  for (int64_t i = 0; i < n_pairs; ++i) est[i] = expected_hits_geo(pairs[i]);
+  double scale = 4.0;
+  int64_t total = 0;
+  for (int64_t start = 0; start < n_pairs;) {
+    int64_t end = start;
+    double acc = 0.0;
+    while (end < n_pairs && (end == start || acc + scale * est[end] <= 0.8 * (double)cap)) acc += scale * est[end++];
+    unsigned long long cnt[4];
+    for (;;) {
+      pp::LaunchArgs a = base_args(c, &o);
+      a.pairs = d_pairs + start;
+      a.n_pairs = end - start;
+      a.pair_base = (uint32_t)start;
+      a.chunk_offsets = static_cast<unsigned long long*>(c->offsets.p);
+      a.queue = static_cast<unsigned long long*>(c->queue.p);
+      a.hits = static_cast<pp_hit*>(c->hits.p);
+      a.hit_cap = (unsigned long long)cap;
+      a.counters = static_cast<unsigned long long*>(c->counters.p);
+      a.stats = static_cast<double*>(c->stats.p) + start * PP_STATS;
+      a.hist = bins > 0 ? static_cast<double*>(c->hist.p) + start * bins : nullptr;
+      const bool whole = start == 0 && end == n_pairs;
+      if ((e = run_batched(c, a, s, whole)) ||
+          (e = cudaMemcpyAsync(cnt, c->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, s)) ||
+          (e = cudaStreamSynchronize(s)))
+        return c->cuda_fail(e, "pp_propagate_fit wave");
+      double wave_est = 0.0;
+      for (int64_t i = start; i < end; ++i) wave_est += est[i];
+      if (wave_est > 0.0) scale = std::max(1.0, 1.25 * (double)cnt[0] / wave_est);
+      if (cnt[0] <= (unsigned long long)cap) break;
+      if (end - start == 1) {
+        *n_hits = (int64_t)cnt[0];
+        return c->fail(PP_ERR_OVERFLOW, "one pair has more hits than hit_capacity; raise hit_capacity");
+      }
+      end = start + (end - start) / 2;
+    }
+    if ((e = pp::launch_fit_moments_hits(c->fitk, c->d_tables, d_pairs, n_pairs, o.mode,
+                                         static_cast<const pp_hit*>(c->hits.p), (unsigned long long)cap,
+                                         static_cast<const unsigned long long*>(c->counters.p),
+                                         static_cast<unsigned long long*>(c->fit_counts.p),
+                                         static_cast<pp::FitRec*>(c->fit_rec.p),
+                                         static_cast<const float2*>(c->fit_cs.p), n_angles, d_mom, c->sm_count, s)))
+      return c->cuda_fail(e, "fit moments");
+    total += (int64_t)cnt[0];
+    start = end;
+  }
+  if ((e = pp::launch_fit_gamma(d_mom, n_pairs, n_angles, d_pairs, 0, static_cast<double*>(c->fit_out.p), s)) ||
       (rows && (e = cudaMemcpyAsync(fits, c->fit_out.p, rows * PP_FIT_OUT * sizeof(double), cudaMemcpyDeviceToHost, s))) ||
       (rows && moments &&
-       (e = cudaMemcpyAsync(moments, c->fit_moments.p, rows * PP_FIT_MOMENTS * sizeof(double), cudaMemcpyDeviceToHost, s))) ||
+       (e = cudaMemcpyAsync(moments, d_mom, rows * PP_FIT_MOMENTS * sizeof(double), cudaMemcpyDeviceToHost, s))) ||
       (n_pairs > 0 && stats &&
        (e = cudaMemcpyAsync(stats, c->stats.p, (size_t)n_pairs * PP_STATS * sizeof(double), cudaMemcpyDeviceToHost, s))) ||
       (n_pairs > 0 && bins > 0 &&
        (e = cudaMemcpyAsync(hist, c->hist.p, (size_t)n_pairs * bins * sizeof(double), cudaMemcpyDeviceToHost, s))) ||
       (e = cudaStreamSynchronize(s)))
     return c->cuda_fail(e, "pp_propagate_fit copy back");
-  *n_hits = (int64_t)cnt[0];
-  if ((int64_t)cnt[0] > cap)
-    return c->fail(PP_ERR_OVERFLOW, "more hits than hit_capacity; the fits cover the stored hits only");
+  *n_hits = total;
   return PP_OK;
 }
 

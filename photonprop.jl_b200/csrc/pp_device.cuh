@@ -449,33 +449,19 @@ __device__ __forceinline__ HitValues hit_values(const DevTables& T, const RunPar
   return h;
 }
 
-// Per-pair FP64 accumulation, histogram and warp-aggregated hit write-back.
-__device__ __forceinline__ void record_hit(const RunParams& R, const PairCtx& c, const Photon& s,
-                                           const HitValues& h, int stats_row) {
-  double* st = R.stats + (int64_t)stats_row * PP_STATS;
-  const double w = (double)h.weight;
-  const double t = (double)h.time;
-  atomicAdd(st + 0, 1.0);
-  atomicAdd(st + 1, w);
-  atomicAdd(st + 2, w * w);
-  atomicAdd(st + 3, w * t);
-  atomicAdd(st + 4, w * t * t);
-  atomicAdd(st + 5, w * (double)logf(h.time));
+// One hit's histogram bin (FP64 atomic).
+__device__ __forceinline__ void histogram_hit(const RunParams& R, const HitValues& h, int stats_row) {
   if (R.hist_bins > 0) {
     const float fb = floorf((h.time - R.hist_t0) * R.inv_bin_width);
     if (fb >= 0.f && fb < (float)R.hist_bins)
-      atomicAdd(R.hist + (int64_t)stats_row * R.hist_bins + (int)fb, w);
+      atomicAdd(R.hist + (int64_t)stats_row * R.hist_bins + (int)fb, (double)h.weight);
   }
-  // warp-aggregated slot reservation among the lanes that hit in this step
-  const unsigned m = __activemask();
-  const int leader = __ffs(m) - 1;
-  const unsigned lane = threadIdx.x & 31u;
-  const unsigned rank = __popc(m & ((1u << lane) - 1u));
-  unsigned long long base = 0;
-  if ((int)lane == leader) base = atomicAdd(R.counters + 0, (unsigned long long)__popc(m));
-  base = __shfl_sync(m, base, leader);
+}
+
+// Writes hit record idx (or flags the overflow).
+__device__ __forceinline__ void write_hit(const RunParams& R, const PairCtx& c, const Photon& s, const HitValues& h,
+                                          unsigned long long idx) {
   if (R.flags & PP_OPT_NO_HITS) return;
-  const unsigned long long idx = base + rank;
   if (idx < R.hit_cap) {
     if (R.flags & PP_OPT_COMPACT_HITS) {
       float4* dst = reinterpret_cast<float4*>(reinterpret_cast<pp_hit32*>(R.hits) + idx);
@@ -493,6 +479,74 @@ __device__ __forceinline__ void record_hit(const RunParams& R, const PairCtx& c,
   } else {
     atomicOr(R.counters + 2, 1ull);
   }
+}
+
+// Per-pair FP64 accumulation, histogram and warp-aggregated hit write-back,
+// called by the lanes that hit (any convergence).
+__device__ __forceinline__ void record_hit(const RunParams& R, const PairCtx& c, const Photon& s,
+                                           const HitValues& h, int stats_row) {
+  double* st = R.stats + (int64_t)stats_row * PP_STATS;
+  const double w = (double)h.weight;
+  const double t = (double)h.time;
+  atomicAdd(st + 0, 1.0);
+  atomicAdd(st + 1, w);
+  atomicAdd(st + 2, w * w);
+  atomicAdd(st + 3, w * t);
+  atomicAdd(st + 4, w * t * t);
+  atomicAdd(st + 5, w * (double)logf(h.time));
+  histogram_hit(R, h, stats_row);
+  // warp-aggregated slot reservation among the lanes that hit in this step
+  const unsigned m = __activemask();
+  const int leader = __ffs(m) - 1;
+  const unsigned lane = threadIdx.x & 31u;
+  const unsigned rank = __popc(m & ((1u << lane) - 1u));
+  unsigned long long base = 0;
+  if ((int)lane == leader) base = atomicAdd(R.counters + 0, (unsigned long long)__popc(m));
+  base = __shfl_sync(m, base, leader);
+  write_hit(R, c, s, h, base + rank);
+}
+
+// A warp's running sums for the pair of its current photon chunk (shared
+// memory): hits of that pair add here and the warp adds the sums to the
+// pair's FP64 statistics when it moves to another pair, so a hit-dense pair
+// does not serialise every hit on its six global addresses.
+struct WarpStats {
+  double v[6];
+  int32_t pair;
+  int32_t pad;
+};
+
+__device__ __forceinline__ void flush_warp_stats(double* stats, WarpStats* ws) {
+  if (ws->pair >= 0 && ws->v[0] != 0.0) {
+    double* st = stats + (int64_t)ws->pair * PP_STATS;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) atomicAdd(st + k, ws->v[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < 6; ++k) ws->v[k] = 0.0;
+}
+
+// record_hit with the warp's statistics cache: lanes whose pair is the
+// cached one add to it (shared-memory atomics), others to the global sums.
+__device__ __forceinline__ void record_hit_cached(const RunParams& R, WarpStats* ws, const PairCtx& c,
+                                                  const Photon& s, const HitValues& h) {
+  const double w = (double)h.weight;
+  const double t = (double)h.time;
+  double* st = c.index == ws->pair ? ws->v : R.stats + (int64_t)c.index * PP_STATS;
+  atomicAdd(st + 0, 1.0);
+  atomicAdd(st + 1, w);
+  atomicAdd(st + 2, w * w);
+  atomicAdd(st + 3, w * t);
+  atomicAdd(st + 4, w * t * t);
+  atomicAdd(st + 5, w * (double)logf(h.time));
+  histogram_hit(R, h, c.index);
+  const unsigned m = __activemask();
+  const int leader = __ffs(m) - 1;
+  const unsigned lane = threadIdx.x & 31u;
+  unsigned long long base = 0;
+  if ((int)lane == leader) base = atomicAdd(R.counters + 0, (unsigned long long)__popc(m));
+  base = __shfl_sync(m, base, leader);
+  write_hit(R, c, s, h, base + __popc(m & ((1u << lane) - 1u)));
 }
 
 }  // namespace ppd

@@ -44,7 +44,10 @@ __global__ void fit_count_kernel(const pp_hit* __restrict__ hits, const unsigned
   for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (unsigned long long)gridDim.x * blockDim.x) {
     const uint32_t p = __ldg(&hits[i].pair);
-    if ((int64_t)p < n_pairs) atomicAdd(counts + p, 1ull);
+    if ((int64_t)p >= n_pairs) continue;
+    // one atomic per pair per warp: hits of one pair sit together in the buffer
+    const unsigned grp = __match_any_sync(__activemask(), p);
+    if ((threadIdx.x & 31u) == (unsigned)(__ffs(grp) - 1)) atomicAdd(counts + p, (unsigned long long)__popc(grp));
   }
 }
 
@@ -129,8 +132,13 @@ __global__ void fit_scatter_kernel(const pp_hit* __restrict__ hits, const unsign
     const float d = sqrtf(fmaf(dx, dx, fmaf(dy, dy, dz * dz)));
     const float tgeo = (d - tg.w) * (mode == kCompat ? K.n800_phase : K.n800_group) / kCVac;
     const float tres = h0.w - (mode == kCompat ? 0.f : pt.w) - tgeo;
-    const unsigned long long slot = atomicAdd(cursor + p, 1ull);
-    write_rec(rec + slot, ct, st, 1.f / n_ph, wn, tres, (int)p);
+    const unsigned grp = __match_any_sync(__activemask(), p);
+    const unsigned lane = threadIdx.x & 31u;
+    const int lead = __ffs(grp) - 1;
+    unsigned long long base = 0;
+    if ((int)lane == lead) base = atomicAdd(cursor + p, (unsigned long long)__popc(grp));
+    base = __shfl_sync(grp, base, lead);
+    write_rec(rec + base + __popc(grp & ((1u << lane) - 1u)), ct, st, 1.f / n_ph, wn, tres, (int)p);
   }
 }
 
@@ -249,22 +257,14 @@ int grid_for(int64_t n, int block, int sm_count) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)sm_count * 8));
 }
 
-cudaError_t moments_and_fits(const FitConsts& K, const FitRec* rec, const unsigned long long* n_ptr,
-                             unsigned long long n_fixed, unsigned long long cap, const float2* cs, int n_angles,
-                             int64_t rows_pairs, const pp_pair* pairs, int64_t n_gen, double* moments, double* fits,
-                             cudaStream_t s) {
-  cudaError_t e;
-  if ((e = cudaMemsetAsync(moments, 0, (size_t)rows_pairs * n_angles * PP_FIT_MOMENTS * sizeof(double), s))) return e;
+cudaError_t add_moments(const FitConsts& K, const FitRec* rec, const unsigned long long* n_ptr,
+                        unsigned long long n_fixed, unsigned long long cap, const float2* cs, int n_angles,
+                        double* moments, cudaStream_t s) {
   const unsigned long long span = n_ptr ? cap : n_fixed;
-  if (span > 0) {
-    const int block = std::min(128, ((n_angles + 31) / 32) * 32);
-    dim3 grid((unsigned)((span + ppd::kFitSeg - 1) / ppd::kFitSeg), (unsigned)((n_angles + block - 1) / block));
-    ppd::fit_moments_kernel<<<grid, block, 0, s>>>(rec, n_ptr, n_fixed, cap, cs, n_angles, K, moments);
-    count_launches(1);
-    if ((e = cudaGetLastError())) return e;
-  }
-  const int64_t rows = rows_pairs * n_angles;
-  ppd::fit_gamma_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(moments, rows, n_angles, pairs, n_gen, fits);
+  if (span == 0) return cudaSuccess;
+  const int block = std::min(128, ((n_angles + 31) / 32) * 32);
+  dim3 grid((unsigned)((span + ppd::kFitSeg - 1) / ppd::kFitSeg), (unsigned)((n_angles + block - 1) / block));
+  ppd::fit_moments_kernel<<<grid, block, 0, s>>>(rec, n_ptr, n_fixed, cap, cs, n_angles, K, moments);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -283,27 +283,34 @@ void fill_fit_consts(FitConsts* K, double n800_phase, double n800_group) {
   for (int i = 0; i < kAngIntN; ++i) K->normf[i] = (float)t[i];
 }
 
-cudaError_t launch_fit_hits(const FitConsts& K, const void* tables, const pp_pair* pairs, int64_t n_pairs, int mode,
-                            const pp_hit* hits, unsigned long long cap, const unsigned long long* counters,
-                            unsigned long long* counts, FitRec* rec, const float2* cs,
-                            int n_angles, double* moments, double* fits, int sm_count, cudaStream_t s) {
+cudaError_t launch_fit_gamma(const double* moments, int64_t n_pairs, int n_angles, const pp_pair* pairs,
+                             int64_t n_gen, double* fits, cudaStream_t s) {
+  const int64_t rows = n_pairs * n_angles;
+  if (rows == 0) return cudaSuccess;
+  ppd::fit_gamma_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(moments, rows, n_angles, pairs, n_gen, fits);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fit_moments_hits(const FitConsts& K, const void* tables, const pp_pair* pairs, int64_t n_pairs,
+                                    int mode, const pp_hit* hits, unsigned long long cap,
+                                    const unsigned long long* counters, unsigned long long* counts, FitRec* rec,
+                                    const float2* cs, int n_angles, double* moments, int sm_count, cudaStream_t s) {
   cudaError_t e;
-  if (n_pairs == 0) return cudaSuccess;
+  if (n_pairs == 0 || cap == 0) return cudaSuccess;
   if ((e = cudaMemsetAsync(counts, 0, (size_t)n_pairs * sizeof(unsigned long long), s))) return e;
-  if (cap > 0) {
-    const int g = grid_for((int64_t)cap, 256, sm_count);
-    ppd::fit_count_kernel<<<g, 256, 0, s>>>(hits, counters, cap, n_pairs, counts);
-    count_launches(1);
-    if ((e = cudaGetLastError())) return e;
-    ppd::fit_scan_kernel<<<1, 1024, 0, s>>>(counts, n_pairs);
-    count_launches(1);
-    if ((e = cudaGetLastError())) return e;
-    ppd::fit_scatter_kernel<<<g, 256, 0, s>>>(hits, counters, cap, pairs, n_pairs, mode,
-                                              static_cast<const ppd::DevTables*>(tables), K, counts, rec);
-    count_launches(1);
-    if ((e = cudaGetLastError())) return e;
-  }
-  return moments_and_fits(K, rec, counters, 0, cap, cs, n_angles, n_pairs, pairs, 0, moments, fits, s);
+  const int g = grid_for((int64_t)cap, 256, sm_count);
+  ppd::fit_count_kernel<<<g, 256, 0, s>>>(hits, counters, cap, n_pairs, counts);
+  count_launches(1);
+  if ((e = cudaGetLastError())) return e;
+  ppd::fit_scan_kernel<<<1, 1024, 0, s>>>(counts, n_pairs);
+  count_launches(1);
+  if ((e = cudaGetLastError())) return e;
+  ppd::fit_scatter_kernel<<<g, 256, 0, s>>>(hits, counters, cap, pairs, n_pairs, mode,
+                                            static_cast<const ppd::DevTables*>(tables), K, counts, rec);
+  count_launches(1);
+  if ((e = cudaGetLastError())) return e;
+  return add_moments(K, rec, counters, 0, cap, cs, n_angles, moments, s);
 }
 
 cudaError_t launch_fit_columns(const FitConsts& K, const void* tables, int64_t n, const double* tres,
@@ -311,14 +318,16 @@ cudaError_t launch_fit_columns(const FitConsts& K, const void* tables, int64_t n
                                FitRec* rec, const float2* cs, int n_angles, int64_t n_gen, double* moments,
                                double* fits, int sm_count, cudaStream_t s) {
   cudaError_t e;
+  if ((e = cudaMemsetAsync(moments, 0, (size_t)n_angles * PP_FIT_MOMENTS * sizeof(double), s))) return e;
   if (n > 0) {
     ppd::fit_columns_kernel<<<grid_for(n, 256, sm_count), 256, 0, s>>>(
         n, tres, theta, ref_ix, abs_w, wl, static_cast<const ppd::DevTables*>(tables), K, rec);
     count_launches(1);
     if ((e = cudaGetLastError())) return e;
+    if ((e = add_moments(K, rec, nullptr, (unsigned long long)n, (unsigned long long)n, cs, n_angles, moments, s)))
+      return e;
   }
-  return moments_and_fits(K, rec, nullptr, (unsigned long long)n, (unsigned long long)n, cs, n_angles, 1, nullptr,
-                          n_gen, moments, fits, s);
+  return launch_fit_gamma(moments, 1, n_angles, nullptr, n_gen, fits, s);
 }
 
 }  // namespace pp

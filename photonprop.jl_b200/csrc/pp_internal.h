@@ -26,6 +26,7 @@ struct LaunchArgs {
   double* hist;
   const void* tables;  // device DevTables
   pp_run_opts opts;
+  uint32_t pair_base;  // added to the pair index written into hits
 };
 
 void count_launches(uint64_t n);
@@ -86,10 +87,15 @@ struct FitRec {  // 32 bytes, one per hit
 };
 static_assert(sizeof(FitRec) == 32, "FitRec is moved as two 16-byte words");
 void fill_fit_consts(FitConsts* K, double n800_phase, double n800_group);
-cudaError_t launch_fit_hits(const FitConsts& K, const void* tables, const pp_pair* pairs, int64_t n_pairs, int mode,
-                            const pp_hit* hits, unsigned long long cap, const unsigned long long* counters,
-                            unsigned long long* counts, FitRec* rec, const float2* cs, int n_angles,
-                            double* moments, double* fits, int sm_count, cudaStream_t s);
+// Adds the moments of the stored hits (their pair fields index `pairs`) to
+// moments [n_pairs x n_angles x 4]; the caller zeroes moments first.
+cudaError_t launch_fit_moments_hits(const FitConsts& K, const void* tables, const pp_pair* pairs, int64_t n_pairs,
+                                    int mode, const pp_hit* hits, unsigned long long cap,
+                                    const unsigned long long* counters, unsigned long long* counts, FitRec* rec,
+                                    const float2* cs, int n_angles, double* moments, int sm_count, cudaStream_t s);
+// Gamma fits and detection fractions of every (pair, angle) from the moments.
+cudaError_t launch_fit_gamma(const double* moments, int64_t n_pairs, int n_angles, const pp_pair* pairs,
+                             int64_t n_gen, double* fits, cudaStream_t s);
 cudaError_t launch_fit_columns(const FitConsts& K, const void* tables, int64_t n, const double* tres,
                                const double* theta, const double* ref_ix, const double* abs_w, const double* wl,
                                FitRec* rec, const float2* cs, int n_angles, int64_t n_gen, double* moments,

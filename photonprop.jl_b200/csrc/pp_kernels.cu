@@ -40,15 +40,22 @@ struct __align__(16) Staged {
 };
 
 template <int MODE, int WARPS>
-__global__ void __launch_bounds__(WARPS * 32) batched_kernel(const RunParams R) {
+__global__ void __launch_bounds__(WARPS * 32, 1024 / (WARPS * 32)) batched_kernel(const RunParams R) {
   __shared__ __align__(16) DevTables T;
   __shared__ Staged stage[WARPS][kStage];
+  __shared__ WarpStats wstats[WARPS];
   stage_tables(T, R.tables);
+  if ((threadIdx.x & 31u) == 0) {
+    WarpStats& w0 = wstats[threadIdx.x >> 5];
+    w0.pair = -1;
+    for (int k = 0; k < 6; ++k) w0.v[k] = 0.0;
+  }
   __syncthreads();
 
   const unsigned lane = threadIdx.x & 31u;
   const unsigned lt_mask = (1u << lane) - 1u;
   Staged* ring = stage[threadIdx.x >> 5];
+  WarpStats* ws = &wstats[threadIdx.x >> 5];
   const unsigned long long total_chunks = R.chunk_offsets[R.n_pairs];
 
   // warp-uniform state: the current chunk and the ring
@@ -103,6 +110,13 @@ __global__ void __launch_bounds__(WARPS * 32) batched_kernel(const RunParams R) 
             break;
           }
           c_pair = __shfl_sync(kFull, p, 0);
+          if (c_pair != ws->pair) {  // the warp's statistics cache follows its chunk
+            if (lane == 0) {
+              flush_warp_stats(R.stats, ws);
+              ws->pair = c_pair;
+            }
+            __syncwarp();
+          }
           c_base = __shfl_sync(kFull, start, 0);
           c_len = (unsigned)(__shfl_sync(kFull, end, 0) - c_base);
           c_next = 0;
@@ -165,10 +179,12 @@ __global__ void __launch_bounds__(WARPS * 32) batched_kernel(const RunParams R) 
     if (__any_sync(kFull, hit)) {
       if (hit) {
         const HitValues h = hit_values<MODE>(T, R, R.pairs + c.index, c, s);
-        record_hit(R, c, s, h, c.index);
+        record_hit_cached(R, ws, c, s, h);
       }
     }
   }
+  __syncwarp();
+  if (lane == 0) flush_warp_stats(R.stats, ws);
   // photon-step count for the roofline
   unsigned long long st = steps;
 #pragma unroll
@@ -452,7 +468,7 @@ static __host__ ppd::RunParams to_params(const LaunchArgs& a) {
   R.chunk_offsets = a.chunk_offsets;
   R.queue = a.queue;
   R.chunk = a.chunk;
-  R.pair_base = 0;
+  R.pair_base = a.pair_base;
   R.hits = a.hits;
   R.hit_cap = a.hit_cap;
   R.counters = a.counters;

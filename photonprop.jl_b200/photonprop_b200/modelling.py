@@ -129,8 +129,10 @@ class FitResult:
 def propagate_fit(propagator: Propagator, pairs, obs_angles, opts: RunOptions | None = None,
                   hit_capacity: int | None = None) -> FitResult:
     """Propagates a batch and fits every (pair, observation angle) on the
-    device (pp_propagate_fit).  The hit capacity defaults to a geometric
-    estimate and is doubled until the hits fit."""
+    device (pp_propagate_fit).  hit_capacity sizes the device hit buffer
+    (96 bytes per hit with the fit records); the library runs the pairs in
+    waves that fit it.  The default is four times the geometric estimate of
+    the hits, between 2^16 and 2^25."""
     opts = opts or RunOptions(mode="compat", pmt_weight=True)
     o = opts.to_c()
     o.hist_bins = 0
@@ -141,7 +143,7 @@ def propagate_fit(propagator: Propagator, pairs, obs_angles, opts: RunOptions | 
         d = np.linalg.norm(pairs["target"].astype(np.float64) - pairs["pos"].astype(np.float64), axis=1)
         r = pairs["radius"].astype(np.float64)
         frac = np.minimum(1.0, r * r / (4.0 * np.maximum(d - r, 1e-3) ** 2))
-        hit_capacity = int(4 * (frac * pairs["n_photons"]).sum()) + 4096
+        hit_capacity = int(min(max(4 * (frac * pairs["n_photons"]).sum(), 1 << 16), 1 << 25))
     fits = np.zeros((n_p, n_a, _lib.FIT_OUT))
     mom = np.zeros((n_p, n_a, _lib.FIT_MOMENTS))
     stats = np.zeros((n_p, 8))
@@ -151,11 +153,25 @@ def propagate_fit(propagator: Propagator, pairs, obs_angles, opts: RunOptions | 
         st = L.pp_propagate_fit(propagator.handle, pairs.ctypes.data, n_p, ctypes.byref(o), angles.ctypes.data, n_a,
                                 hit_capacity, ctypes.byref(n_hits), fits.ctypes.data, mom.ctypes.data,
                                 stats.ctypes.data, None)
-        if st == _lib.PP_ERR_OVERFLOW:
-            hit_capacity = max(2 * hit_capacity, int(n_hits.value * 1.1) + 1)
+        if st == _lib.PP_ERR_OVERFLOW:  # one pair alone has more hits than the buffer
+            hit_capacity = int(n_hits.value * 1.1) + 1
             continue
         _lib.check(st, propagator.handle)
         return FitResult(fits, mom, stats, int(n_hits.value))
+
+
+def fit_pairs(n_photons_per_dist: int, n_distances: int, n_angles: int, max_dist: float = 300.0, seed: int = 0):
+    """The sample points of make_photon_fits (src/modelling.jl:88-95):
+    (pairs, distances, obs_angles).  Distances are 10^Sobol([0, log10 max_dist])
+    rounded to Float32 like propagate_distance's argument; one isotropic
+    source at the origin and a 0.21 m sphere at (0, 0, distance) per distance."""
+    s = SobolSeq(0.0, np.pi)
+    s2 = SobolSeq(0.0, float(np.float32(np.log10(np.float32(max_dist)))))
+    distances = np.array([np.float32(10.0 ** s2.next()) for _ in range(n_distances)], dtype=np.float32)
+    obs_angles = np.array([s.next() for _ in range(n_angles)])
+    pairs = np.concatenate([point_source_pair(n_photons_per_dist, target=(0.0, 0.0, float(d)), radius=0.21,
+                                              seed=pair_seed(seed, i)) for i, d in enumerate(distances)])
+    return pairs, distances, obs_angles
 
 
 def make_photon_fits(n_photons_per_dist: int, n_distances: int, n_angles: int, max_dist: float = 300.0, *,
@@ -163,20 +179,14 @@ def make_photon_fits(n_photons_per_dist: int, n_distances: int, n_angles: int, m
                      g: float | None = None):
     """make_photon_fits(n_photons_per_dist, n_distances, n_angles, max_dist),
     src/modelling.jl:86-111: distances 10^Sobol([0, log10 max_dist]) and
-    observation angles Sobol([0, pi]); an isotropic source at the origin and
-    a 0.21 m sphere at (0, 0, distance) per distance (propagate_distance);
-    all distances propagate in one batched launch and every (distance, angle)
-    is fitted on the device.  Returns the DataFrame
-    (obs_angle, fit_alpha, fit_theta, det_fraction, distance), distances
-    outer, angles inner, as the reference's vcat(..., source=:distance)."""
+    observation angles Sobol([0, pi]) (fit_pairs); all distances propagate in
+    one batched launch and every (distance, angle) is fitted on the device.
+    Returns the DataFrame (obs_angle, fit_alpha, fit_theta, det_fraction,
+    distance), distances outer, angles inner, as the reference's
+    vcat(..., source=:distance)."""
     import pandas as pd
     prop = propagator or _default_propagator()
-    s = SobolSeq(0.0, np.pi)
-    s2 = SobolSeq(0.0, float(np.float32(np.log10(np.float32(max_dist)))))
-    distances = np.array([np.float32(10.0 ** s2.next()) for _ in range(n_distances)], dtype=np.float32)
-    obs_angles = np.array([s.next() for _ in range(n_angles)])
-    pairs = np.concatenate([point_source_pair(n_photons_per_dist, target=(0.0, 0.0, float(d)), radius=0.21,
-                                              seed=pair_seed(seed, i)) for i, d in enumerate(distances)])
+    pairs, distances, obs_angles = fit_pairs(n_photons_per_dist, n_distances, n_angles, max_dist, seed)
     res = propagate_fit(prop, pairs, obs_angles, RunOptions(mode=mode, g=g, pmt_weight=True, hist_bins=0))
     f = res.fits.reshape(-1, _lib.FIT_OUT)
     return pd.DataFrame({"obs_angle": np.tile(obs_angles, n_distances), "fit_alpha": f[:, 0], "fit_theta": f[:, 1],

@@ -137,3 +137,16 @@ def test_make_photon_fits_table(propagator, tmp_path):
     md.write_fit_table(df, tmp_path / "fits.parquet")
     back = md.read_parquet(tmp_path / "fits.parquet")
     np.testing.assert_array_equal(back.to_numpy(), df.to_numpy())
+
+
+def test_waves_match_one_launch(propagator):
+    pairs = np.concatenate([pp.batches.point_source_pair(1_000_000, target=(0.0, 0.0, 3.0),
+                                                         seed=pp.propagation.pair_seed(11, i)) for i in range(8)])
+    ro = pp.RunOptions(mode="compat", pmt_weight=True, hist_bins=0)
+    one = md.propagate_fit(propagator, pairs, ANGLES, ro, hit_capacity=1 << 21)
+    assert one.n_hits < 1 << 21
+    waves = md.propagate_fit(propagator, pairs, ANGLES, ro, hit_capacity=one.n_hits // 3)
+    assert waves.n_hits == one.n_hits
+    np.testing.assert_allclose(waves.stats, one.stats, rtol=1e-9)
+    np.testing.assert_allclose(waves.moments, one.moments, rtol=1e-9)
+    np.testing.assert_allclose(waves.fits, one.fits, rtol=1e-7)
