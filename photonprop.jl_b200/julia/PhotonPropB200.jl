@@ -12,7 +12,7 @@
 module PhotonPropB200
 
 export PPMediumDesc, PPSpectrumDesc, PPPmtDesc, PPPair, PPRunOpts, PPHit
-export Context, propagate_pairs, propagate_distance, default_opts
+export Context, propagate_pairs, propagate_distance, default_opts, make_photon_fits, get_dir_reweight
 
 const libpp = get(ENV, "PHOTONPROP_B200_LIB",
                   joinpath(@__DIR__, "..", "libphotonprop_b200.so"))
@@ -180,6 +180,55 @@ function propagate_distance(ctx::Context, medium::PPMediumDesc, distance::Real, 
     tgeo = (distance - r) / (C_VAC / n800)
     (tres=d ./ (C_VAC ./ ref_ix) .- tgeo, initial_theta=[acos(clamp(Float64(h.dir0[3]), -1, 1)) for h in hits],
      ref_ix=ref_ix, abs_weight=exp.(-d ./ labs), dist_travelled=d, wavelength=wl)
+end
+
+"""
+    sobol_1d(lb, ub, n)
+
+The first n points of Sobol.jl's one-dimensional `SobolSeq([lb], [ub])`
+(the bit-reversed Gray code of k = 1, 2, ...).
+"""
+sobol_1d(lb, ub, n) = [lb + (ub - lb) * bitreverse(UInt32(k ⊻ (k >> 1))) / 2.0^32 for k in 1:n]
+
+"""
+    make_photon_fits(ctx, n_photons_per_dist, n_distances, n_angles, max_dist=300f0; seed=0)
+
+`make_photon_fits` of src/modelling.jl:86-111 as one library call
+(`pp_propagate_fit`): every distance propagates in one batched launch and
+every (distance, angle) is reweighted and fitted on the device.  Returns a
+NamedTuple of the reference's DataFrame columns.
+"""
+function make_photon_fits(ctx::Context, n_photons_per_dist::Integer, n_distances::Integer, n_angles::Integer,
+                          max_dist::Real=300f0; seed::Integer=0, hit_capacity::Integer=1 << 25)
+    distances = Float32.(10 .^ sobol_1d(0.0, Float64(Float32(log10(Float32(max_dist)))), n_distances))
+    obs_angles = sobol_1d(0.0, Float64(pi), n_angles)
+    pairs = [PPPair((0f0, 0f0, 0f0), 0f0, (0f0, 0f0, 1f0), 0f0, (0f0, 0f0, d), 0.21f0, Int64(n_photons_per_dist),
+                    ccall((:pp_pair_seed, libpp), UInt64, (UInt64, UInt64), UInt64(seed), UInt64(i - 1)),
+                    PP_EMITTER_ISOTROPIC, (Int32(0), Int32(0), Int32(0))) for (i, d) in enumerate(distances)]
+    o = default_opts(PP_MODE_COMPAT)
+    opts = PPRunOpts(o.mode, o.max_steps, o.g, o.t_max, o.hist_t0, o.hist_bin_width, Int32(0),
+                     o.flags | PP_OPT_PMT_WEIGHT, o.block_size, o.blocks_per_sm, o.chunk_photons, o.reserved)
+    fits = Array{Cdouble}(undef, 3, n_angles, n_distances)
+    nh = Ref{Int64}(0)
+    check(ccall((:pp_propagate_fit, libpp), Cint,
+                (Ptr{Cvoid}, Ptr{PPPair}, Int64, Ref{PPRunOpts}, Ptr{Cdouble}, Int32, Int64, Ref{Int64},
+                 Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}, Ptr{Cdouble}),
+                ctx.ptr, pairs, n_distances, opts, obs_angles, n_angles, hit_capacity, nh, fits, C_NULL, C_NULL,
+                C_NULL), ctx.ptr)
+    (obs_angle=repeat(obs_angles, n_distances), fit_alpha=vec(fits[1, :, :]), fit_theta=vec(fits[2, :, :]),
+     det_fraction=vec(fits[3, :, :]), distance=repeat(Float64.(distances), inner=n_angles))
+end
+
+"""
+    get_dir_reweight(thetas, obs_angle, ref_ixs)
+
+src/modelling.jl:46-49 through the library's FP64 host function.
+"""
+function get_dir_reweight(thetas::AbstractVector{Float64}, obs_angle::Real, ref_ixs::AbstractVector{Float64})
+    out = similar(thetas)
+    check(ccall((:pp_dir_reweight, libpp), Cint, (Ptr{Cdouble}, Cdouble, Ptr{Cdouble}, Ptr{Cdouble}, Int64),
+                thetas, obs_angle, ref_ixs, out, length(thetas)))
+    out
 end
 
 end # module
