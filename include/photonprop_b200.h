@@ -336,6 +336,62 @@ PP_API pp_status pp_fit_photon_dist_device(pp_ctx* ctx, int64_t n, const double*
                                            const double* obs_angles, int32_t n_angles, int64_t n_ph_gen,
                                            double* d_moments, double* d_fits, void* stream);
 
+/* ---- light yield: particles -> light sources (src/lightyield.jl) -------- */
+enum { PP_PARTICLE_EMINUS = 11, PP_PARTICLE_EPLUS = -11, PP_PARTICLE_GAMMA = 22 };
+/* Particle, src/lightyield.jl:201-207: position (m), time (ns), direction
+ * (unit), energy (GeV), type (PP_PARTICLE_*).  48 bytes. */
+typedef struct {
+  float pos[3];
+  float time;
+  float dir[3];
+  float energy;
+  int32_t type;
+  int32_t reserved[3];
+} pp_particle;
+/* Units of the longitudinal grid.  PP_LY_REFERENCE reproduces the
+ * reference's arithmetic: grid values are centimetres in the shower profile
+ * and are used unchanged as metres for the source positions and times
+ * (src/lightyield.jl:253-256), and the water density is the reference's
+ * expression A / B^((1 + (1 - T)/C)^D) with T in degC (src/medium.jl:78).
+ * PP_LY_METRES takes the grid in metres (converted to centimetres for the
+ * profile) and the DIPPR105 density A / B^(1 + (1 - T/C)^D), T in kelvin. */
+enum { PP_LY_REFERENCE = 0, PP_LY_METRES = 1 };
+/* density(medium) in kg/m^3 (src/medium.jl:69-92) */
+PP_API double pp_medium_density(const pp_medium_desc* m, int32_t ly_mode);
+/* longitudinal_profile(energy, z, medium, ptype), src/lightyield.jl:116-140:
+ * energy in GeV, z in cm; per cm. */
+PP_API double pp_longitudinal_profile(const pp_medium_desc* m, int32_t ly_mode, int32_t ptype, double energy_gev,
+                                      double z_cm);
+/* cherenkov_track_length(_dev), src/lightyield.jl:190-198 (cm); NaN for an unknown type. */
+PP_API double pp_cherenkov_track_length(int32_t ptype, double energy_gev);
+PP_API double pp_cherenkov_track_length_dev(int32_t ptype, double energy_gev);
+/* frank_tamm_norm(wl_range, n(medium)), src/spectrum.jl:41-45: Cherenkov photons per cm of track. */
+PP_API double pp_frank_tamm_norm(const pp_medium_desc* m, double wl_min, double wl_max);
+/* fractional_contrib_long!(energy, z_grid, medium, ptype, out),
+ * src/lightyield.jl:143-169: out[0] = 0, out[i] = the profile's share of
+ * [z[i-1], z[i]] (50-point Gauss-Legendre over each interval and over the
+ * whole grid); z in cm. */
+PP_API pp_status pp_fractional_contrib_long(const pp_medium_desc* m, int32_t ly_mode, int32_t ptype,
+                                            double energy_gev, const double* z_grid_cm, int64_t n, double* out);
+/* particle_to_elongated_lightsource for n_particles particles on the device
+ * (src/lightyield.jl:219-285): the grid len_min:precision:len_max (n_grid
+ * points, Julia's range) gives n_grid - 1 sources per particle at the
+ * interval midpoints, with round(frank_tamm_norm(wl_range) x
+ * cherenkov_track_length(E) x fractional share) photons, written as pairs
+ * (position, time, direction, photons, `emitter`; target and seed unset):
+ * source k of particle p is d_sources[p * (n_grid - 1) + k].  An isotropic
+ * source sits at the midpoint; a Cherenkov-cone source is a track over its
+ * interval along the particle.  n_grid comes back in *n_grid. */
+PP_API pp_status pp_particles_to_sources_device(pp_ctx* ctx, const pp_particle* d_particles, int64_t n_particles,
+                                                double len_min, double len_max, double precision, int32_t ly_mode,
+                                                double wl_min, double wl_max, int32_t emitter, pp_pair* d_sources,
+                                                int64_t capacity, int64_t* n_grid, void* stream);
+/* Every source with every target sphere (d_targets: x, y, z, radius floats):
+ * d_pairs[s * n_targets + t], seed pp_pair_seed(seed, s * n_targets + t). */
+PP_API pp_status pp_cross_pairs_device(pp_ctx* ctx, const pp_pair* d_sources, int64_t n_sources,
+                                       const float* d_targets, int64_t n_targets, uint64_t seed, pp_pair* d_pairs,
+                                       void* stream);
+
 /* ---- serving: continuous batching ----------------------------------------- */
 /* A request is a list of pairs.  A scheduler thread admits waiting requests
  * while their hit buffers fit the HBM budget (bytes_per_hit per expected hit)

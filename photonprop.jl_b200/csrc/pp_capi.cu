@@ -1055,6 +1055,10 @@ pp_status propagate_with_scratch(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pa
 
 int ctx_device(const pp_ctx* c) { return c->device; }
 int ctx_sm_count(const pp_ctx* c) { return c->sm_count; }
+const pp_medium_desc* ctx_medium(const pp_ctx* c) { return &c->medium; }
+pp_status ctx_fail(pp_ctx* c, pp_status s, const char* msg) { return c->fail(s, msg); }
+pp_status ctx_cuda_fail(pp_ctx* c, cudaError_t e, const char* where) { return c->cuda_fail(e, where); }
+std::mutex& ctx_mutex(pp_ctx* c) { return c->mu; }
 }  // namespace pp
 
 // ---------------------------------------------------------------------------

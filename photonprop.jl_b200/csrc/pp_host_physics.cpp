@@ -100,6 +100,21 @@ double frank_tamm_norm(const pp_medium_desc* m, double a, double b, const std::v
 
 namespace pp {
 
+void gl_nodes(int n, double* x, double* w) {
+  std::vector<double> xv, wv;
+  gauss_legendre(n, xv, wv);
+  for (int i = 0; i < n; ++i) {
+    x[i] = xv[i];
+    w[i] = wv[i];
+  }
+}
+
+double frank_tamm_norm_cm(const pp_medium_desc* m, double wl_min, double wl_max) {
+  std::vector<double> x, w;
+  gauss_legendre(50, x, w);
+  return frank_tamm_norm(m, wl_min, wl_max, x, w);
+}
+
 void medium_coeffs(const pp_medium_desc* m, double out[11]) {
   double a01, a2, a3, a4;
   fry(m, a01, a2, a3, a4);

@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 
 #include "photonprop_b200.h"
 
@@ -60,6 +61,10 @@ pp_status propagate_with_scratch(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pa
                                  cudaStream_t stream);
 int ctx_device(const pp_ctx* c);
 int ctx_sm_count(const pp_ctx* c);
+const pp_medium_desc* ctx_medium(const pp_ctx* c);
+pp_status ctx_fail(pp_ctx* c, pp_status s, const char* msg);
+pp_status ctx_cuda_fail(pp_ctx* c, cudaError_t e, const char* where);
+std::mutex& ctx_mutex(pp_ctx* c);
 
 // Cherenkov angular distribution of EM cascades, e- parameters
 // (src/emission.jl:19), and the reference's table of its [-1, 1] integral
@@ -102,6 +107,8 @@ cudaError_t launch_fit_columns(const FitConsts& K, const void* tables, int64_t n
                                double* fits, int sm_count, cudaStream_t s);
 
 // host physics (pp_host_physics.cpp)
+void gl_nodes(int n, double* x, double* w);  // Gauss-Legendre nodes and weights on [-1, 1]
+double frank_tamm_norm_cm(const pp_medium_desc* m, double wl_min, double wl_max);  // photons per cm
 void medium_coeffs(const pp_medium_desc* m, double out[11]);
 void default_abs_table(double* wl, double* len, int* n);
 

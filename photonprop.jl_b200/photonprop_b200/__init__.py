@@ -20,6 +20,7 @@ from . import serving
 from . import parallel
 from . import surrogate
 from . import modelling
+from . import lightyield
 
 
 def build(force=False):

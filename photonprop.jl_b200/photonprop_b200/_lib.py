@@ -133,6 +133,15 @@ _SIGS = [
     ("pp_fit_hits_device", ctypes.c_int, [_VP, _VP, _I64, _I32, _VP, _I64, _VP, _VP, _I32, _VP, _VP, _VP]),
     ("pp_fit_photon_dist_device", ctypes.c_int, [_VP, _I64, _VP, _VP, _VP, _VP, _VP, _VP, _I32, _I64, _VP, _VP,
                                                  _VP]),
+    ("pp_medium_density", _D, [ctypes.POINTER(MediumDesc), _I32]),
+    ("pp_longitudinal_profile", _D, [ctypes.POINTER(MediumDesc), _I32, _I32, _D, _D]),
+    ("pp_cherenkov_track_length", _D, [_I32, _D]),
+    ("pp_cherenkov_track_length_dev", _D, [_I32, _D]),
+    ("pp_frank_tamm_norm", _D, [ctypes.POINTER(MediumDesc), _D, _D]),
+    ("pp_fractional_contrib_long", ctypes.c_int, [ctypes.POINTER(MediumDesc), _I32, _I32, _D, _VP, _I64, _VP]),
+    ("pp_particles_to_sources_device", ctypes.c_int, [_VP, _VP, _I64, _D, _D, _D, _I32, _D, _D, _I32, _VP, _I64,
+                                                      ctypes.POINTER(_I64), _VP]),
+    ("pp_cross_pairs_device", ctypes.c_int, [_VP, _VP, _I64, _VP, _I64, ctypes.c_uint64, _VP, _VP]),
     ("pp_server_create", ctypes.c_int, [_VP, ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
     ("pp_server_destroy", None, [_VP]),
     ("pp_server_submit", ctypes.c_int, [_VP, _VP, _I32, ctypes.POINTER(ctypes.c_uint64)]),
@@ -161,6 +170,11 @@ _SIGS = [
 ]
 
 EXPORTED = [s[0] for s in _SIGS]
+
+PARTICLE_DTYPE = np.dtype([("pos", "<f4", 3), ("time", "<f4"), ("dir", "<f4", 3), ("energy", "<f4"),
+                           ("type", "<i4"), ("reserved", "<i4", 3)])
+assert PARTICLE_DTYPE.itemsize == 48
+LY_REFERENCE, LY_METRES = 0, 1
 
 FIT_MOMENTS = 4
 FIT_OUT = 3

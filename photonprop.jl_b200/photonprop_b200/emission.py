@@ -49,7 +49,14 @@ ANG_DIST_PARS = (4.27033, -6.02527, 0.29887, -0.00103)
 
 
 def cherenkov_ang_dist(costheta, ref_index, pars=ANG_DIST_PARS):
-    """cherenkov_ang_dist, src/emission.jl:32-44 (arXiv:1210.5140)."""
+    """cherenkov_ang_dist, src/emission.jl:32-44 (arXiv:1210.5140); the
+    library's FP64 host function for the e- parameters, the same formula for
+    other parameters."""
+    if tuple(pars) == ANG_DIST_PARS:
+        L = _lib.load()
+        out = np.vectorize(lambda c, n: L.pp_cherenkov_ang_dist(float(c), float(n)), otypes=[np.float64])(
+            costheta, ref_index)
+        return float(out) if np.ndim(out) == 0 else out
     a, b, c, d = pars
     ctc = 1.0 / np.asarray(ref_index, dtype=np.float64)
     return a * np.exp(b * np.abs(np.asarray(costheta, dtype=np.float64) - ctc) ** c) + d
