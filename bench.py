@@ -58,7 +58,7 @@ def parse():
                     help="length of the serving sample in the default run (0 = skip)")
     ap.add_argument("--serving-rate", type=float, default=200.0, help="request arrival rate, Hz")
     ap.add_argument("--workload", choices=["batch", "serving", "surrogate", "surrogate-infer", "cone-grid", "point",
-                                           "fits", "event"], default="batch")
+                                           "fits", "event", "llh"], default="batch")
     ap.add_argument("--fit-photons", type=int, default=100_000_000, help="fits workload: photons per distance")
     ap.add_argument("--fit-distances", type=int, default=250)
     ap.add_argument("--fit-angles", type=int, default=250)
@@ -561,6 +561,84 @@ def run_event(args):
     print(json.dumps(line), flush=True)
 
 
+def run_llh(args):
+    """--workload llh: the event of --workload event (100 GeV e-, 200 cone
+    sources x 500 modules) observed once by the MC kernel (each weighted hit
+    kept with probability = its weight), per-(source, module) hypothesis
+    parameters from an independent MC run (expected photons + Gamma-mixture
+    fit of each pair), then the extended likelihood of 64 energy hypotheses
+    per launch on the device.  Reported: hypotheses/s of the likelihood
+    kernel, the surrogate's cost of producing one hypothesis's parameters
+    (1e5 queries), and the MC kernel's time for one hypothesis."""
+    import torch
+    import photonprop_b200 as pp
+    from photonprop_b200 import event as ev
+    from photonprop_b200 import lightyield as ly
+    from photonprop_b200 import surrogate as sg
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    medium = pp.make_seawater(35.0, 2.0)
+    spec = pp.CherenkovSpectrum((300.0, 800.0), 20, medium)
+    xs = np.arange(-40.0, 40.1, 20.0)
+    mods = np.array([[x, y, z, 0.21] for x in xs for y in xs for z in np.arange(-40.0, 55.1, 5.0)],
+                    dtype=np.float32)
+    part = ly.Particle((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), 0.0, 100.0, ly.ParticleType.EMinus)
+    ro = pp.RunOptions(mode="physical", g=0.95, t_max=1000.0, hist_bins=1000)
+    with pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=0) as prop:
+        src, _ = ly.particles_to_sources(prop, [part], (0.0, 20.0), 0.1, mode="metres", emitter="cone")
+        S, M = len(src), len(mods)
+        obs_pairs = ly.cross_pairs(prop, src, mods, seed=11)
+        t0 = time.perf_counter()
+        res = prop.propagate(obs_pairs, pp.RunOptions(mode="physical", g=0.95, t_max=1000.0, hist_bins=0),
+                             hit_capacity=1 << 22)
+        t_mc = time.perf_counter() - t0
+        keep = np.random.default_rng(0).uniform(size=len(res.hits)) < res.hits["weight"]
+        res.hits = res.hits[keep]
+        times = ev.mc_hit_times(res, S, M)
+        hyp_pairs = ly.cross_pairs(prop, src, mods, seed=12)
+        ds = sg.mc_dataset(prop, hyp_pairs, ro, min_hits_mu=0, min_hits_fit=0)
+        y = ds.y.astype(np.float64)
+        prm = np.stack([ds.mu, 1 / (1 + np.exp(-y[:, 1])), np.exp(y[:, 2]), np.exp(y[:, 3]), np.exp(y[:, 4]),
+                        sg.time_shift(hyp_pairs, medium) + hyp_pairs["t0"]], axis=1)
+        prm = np.nan_to_num(prm.reshape(S, M, 6).transpose(1, 0, 2), nan=1.0)
+        H = 64
+        scales = np.geomspace(0.5, 2.0, H)
+        hyp = np.repeat(prm[None], H, axis=0)
+        hyp[..., 0] *= scales[:, None, None]
+        counts = np.array([len(t) for t in times], dtype=np.int64)
+        offs = np.concatenate([[0], np.cumsum(counts)])
+        d_p = torch.from_numpy(np.ascontiguousarray(hyp)).to(dev)
+        d_o = torch.from_numpy(offs).to(dev)
+        d_t = torch.from_numpy(np.concatenate(times)).to(dev)
+        d_l = torch.zeros((H, M), dtype=torch.float64, device=dev)
+        L = pp._lib.load()
+        st = torch.cuda.current_stream(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        tl = []
+        for _ in range(4):
+            e0.record(st)
+            pp._lib.check(L.pp_event_llh_device(prop.handle, pp._lib.LLH_SHIFTED, H, S, M, d_p.data_ptr(), None,
+                                                d_o.data_ptr(), d_t.data_ptr(), d_l.data_ptr(), st.cuda_stream),
+                          prop.handle)
+            e1.record(st)
+            torch.cuda.synchronize()
+            tl.append(e0.elapsed_time(e1) / 1e3)
+        llh = d_l.cpu().numpy().sum(axis=1)
+        inf = surrogate_inference_rate(0, S * M)
+    t_llh = float(np.median(tl[1:]))
+    per_hyp = t_llh / H + S * M / inf["queries_per_s"]
+    line = {"metric": "event likelihood hypotheses/s (surrogate parameters + FP64 likelihood kernel)",
+            "value": 1.0 / per_hyp, "unit": "hypotheses/s", "n_gpus": 1, "higher_is_better": True,
+            "data": "synthetic",
+            "config": {"workload": f"100 GeV e- cascade, {S} cone sources x {M} modules, {int(counts.sum())} "
+                                   f"observed hits, {H} energy hypotheses per launch (x0.5 .. x2)"},
+            "llh_kernel_s_per_launch": t_llh, "llh_hypotheses_per_s": H / t_llh,
+            "surrogate_queries_per_hypothesis": S * M, "surrogate_queries_per_s": inf["queries_per_s"],
+            "mc_seconds_per_hypothesis": t_mc, "speedup_vs_mc": t_mc / per_hyp,
+            "best_scale": float(scales[int(np.argmax(llh))])}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -825,6 +903,8 @@ def main():
         run_fits(args)
     elif args.workload == "event":
         run_event(args)
+    elif args.workload == "llh":
+        run_llh(args)
     elif args.workload == "surrogate-infer":
         import torch
         torch.cuda.set_device(0)

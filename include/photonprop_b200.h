@@ -392,6 +392,29 @@ PP_API pp_status pp_cross_pairs_device(pp_ctx* ctx, const pp_pair* d_sources, in
                                        const float* d_targets, int64_t n_targets, uint64_t seed, pp_pair* d_pairs,
                                        void* stream);
 
+/* ---- event likelihood: Poisson x arrival-time mixture per module -------- */
+/* The extended likelihood of example_full.jl:338-449 for n_hyp hypotheses
+ * of one event at once, one block per (hypothesis, module).  Per source j
+ * and module k, d_params[((h * n_modules + k) * n_sources + j) * PP_LLH_PARAMS]
+ * (module-major: a module's sources are contiguous) holds
+ * (A, w, alpha1, alpha2, theta, t_shift): the expected photons are
+ * mu_jk = A x N_j (N_j = d_source_photons[h * n_sources + j], or 1 when that
+ * pointer is NULL) and the arrival-time density is
+ *   g_jk(x) = w Gamma(x - t_shift; alpha1, theta) + (1 - w) Gamma(x - t_shift; alpha2, theta).
+ * With mu_k = sum_j mu_jk and the module's hit times x (CSR: d_hit_offsets
+ * [n_modules + 1] into d_hit_times),
+ *   llh_k = n_k ln mu_k - mu_k - ln n_k! + sum_x ln(sum_j q_jk g_jk(x)),
+ * q_jk = mu_jk / mu_k (PP_LLH_SHIFTED), or q_jk = A_jk / sum_j A_jk
+ * (PP_LLH_REFERENCE: shape_mixture_per_module weighs the sources by their
+ * detection fraction alone, example_full.jl:362-377).  FP64 throughout;
+ * d_llh[h * n_modules + k]. */
+#define PP_LLH_PARAMS 6
+enum { PP_LLH_REFERENCE = 0, PP_LLH_SHIFTED = 1 };
+PP_API pp_status pp_event_llh_device(pp_ctx* ctx, int32_t mode, int64_t n_hyp, int64_t n_sources, int64_t n_modules,
+                                     const double* d_params, const double* d_source_photons,
+                                     const int64_t* d_hit_offsets, const double* d_hit_times, double* d_llh,
+                                     void* stream);
+
 /* ---- serving: continuous batching ----------------------------------------- */
 /* A request is a list of pairs.  A scheduler thread admits waiting requests
  * while their hit buffers fit the HBM budget (bytes_per_hit per expected hit)

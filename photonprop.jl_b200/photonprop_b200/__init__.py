@@ -21,6 +21,7 @@ from . import parallel
 from . import surrogate
 from . import modelling
 from . import lightyield
+from . import event
 
 
 def build(force=False):

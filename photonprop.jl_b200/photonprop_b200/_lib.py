@@ -142,6 +142,7 @@ _SIGS = [
     ("pp_particles_to_sources_device", ctypes.c_int, [_VP, _VP, _I64, _D, _D, _D, _I32, _D, _D, _I32, _VP, _I64,
                                                       ctypes.POINTER(_I64), _VP]),
     ("pp_cross_pairs_device", ctypes.c_int, [_VP, _VP, _I64, _VP, _I64, ctypes.c_uint64, _VP, _VP]),
+    ("pp_event_llh_device", ctypes.c_int, [_VP, _I32, _I64, _I64, _I64, _VP, _VP, _VP, _VP, _VP, _VP]),
     ("pp_server_create", ctypes.c_int, [_VP, ctypes.POINTER(ServerConfig), ctypes.POINTER(_VP)]),
     ("pp_server_destroy", None, [_VP]),
     ("pp_server_submit", ctypes.c_int, [_VP, _VP, _I32, ctypes.POINTER(ctypes.c_uint64)]),
@@ -175,6 +176,8 @@ PARTICLE_DTYPE = np.dtype([("pos", "<f4", 3), ("time", "<f4"), ("dir", "<f4", 3)
                            ("type", "<i4"), ("reserved", "<i4", 3)])
 assert PARTICLE_DTYPE.itemsize == 48
 LY_REFERENCE, LY_METRES = 0, 1
+LLH_PARAMS = 6
+LLH_REFERENCE, LLH_SHIFTED = 0, 1
 
 FIT_MOMENTS = 4
 FIT_OUT = 3
