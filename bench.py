@@ -860,7 +860,9 @@ def run_ours(args):
                      "traffic": roofline.NCU_DRAM_BYTES_PER_PHOTON * photons_local[0],
                      "traffic_note": "DRAM bytes per launch: ncu capture of a 2.5e8-photon launch scaled by photons",
                      "issue_active_ncu": roofline.NCU_ISSUE_ACTIVE,
-                     "note": "issue-bound: ncu shows 79% of issue slots busy (ALU pipe 54%, FMA 34%, XU 27%)",
+                     "note": "issue-bound: ncu shows {:.0%} of issue slots busy (ALU pipe {:.0%}, FMA {:.0%}, XU {:.0%})".format(
+                         roofline.NCU_ISSUE_ACTIVE, roofline.NCU_PIPES["alu"], roofline.NCU_PIPES["fma"],
+                         roofline.NCU_PIPES["xu"]),
                      "peak_source": "measured live: ex2.approx dependent chains over every SM (pp_measure_peaks)",
                      "fp32": {"achieved": a_fp32 / 1e9, "peak": peaks["fp32_ops"] / 1e9, "frac": f_fp32},
                      "philox": {"achieved_blocks_per_s": a_int, "peak_blocks_per_s": peaks["philox_blocks"],

@@ -31,9 +31,10 @@ def op_counts(steps, photons_iso, photons_cone):
 
 # DRAM traffic of the batched kernel per photon, measured with ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on one launch of 2.524e8
-# photons (512 mixed pairs, <= 1e6 photons each): 113.7 KB read, 0 B written.
+# photons (512 mixed pairs, <= 1e6 photons each): 118.0 KB read, 0 B written.
 # Hit records and FP64 histogram reductions stay in L2 during a launch, so
 # the traffic grows with the photon count; bench.py scales it to its launch.
-NCU_DRAM_BYTES_PER_PHOTON = 113.664e3 / 252387747
+NCU_DRAM_BYTES_PER_PHOTON = 118.016e3 / 252387747
 # Issue slots busy in the same capture (smsp__issue_active).
-NCU_ISSUE_ACTIVE = 0.790
+NCU_ISSUE_ACTIVE = 0.793
+NCU_PIPES = {"alu": 0.526, "fma": 0.355, "xu": 0.280}  # pipe utilisation, same capture
