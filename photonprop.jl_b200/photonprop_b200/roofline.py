@@ -38,3 +38,4 @@ NCU_DRAM_BYTES_PER_PHOTON = 118.016e3 / 252387747
 # Issue slots busy in the same capture (smsp__issue_active).
 NCU_ISSUE_ACTIVE = 0.793
 NCU_PIPES = {"alu": 0.526, "fma": 0.355, "xu": 0.280}  # pipe utilisation, same capture
+NCU_BRANCH_UNIFORM = 0.910  # smsp__sass_average_branch_targets_threads_uniform, same capture

@@ -130,6 +130,27 @@ def test_surrogate_trains_and_falls_back_to_mc(propagator):
     x = test.x[good][:8].copy()
     x[:, 2] = 5.0
     np.testing.assert_allclose(s.predict_features(x)[:, 0], pred[:8, 0] / 10.0, rtol=1e-5)
+    # what the network gains over the MC method: its query rate at >= 1000x
+    import time
+    import torch
+    n_q = 1_000_000
+    xq = np.repeat(test.x, n_q // len(test.x) + 1, axis=0)[:n_q]
+    d_x = torch.from_numpy(np.ascontiguousarray(xq)).cuda()
+    d_o = torch.empty((5, n_q), dtype=torch.float32, device="cuda")
+    s.net.forward(d_x, d_o, n_q, physical=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        s.net.forward(d_x, d_o, n_q, physical=True)
+    e1.record()
+    torch.cuda.synchronize()
+    nn_rate = 5 * n_q / (e0.elapsed_time(e1) / 1e3)
+    t0 = time.perf_counter()
+    sg.mc_dataset(propagator, sg.training_pairs(256, 1_000_000, seed=14, d_min=2.0, d_max=10.0), opts,
+                  min_hits_mu=0, min_hits_fit=0)
+    mc_rate = 256 / (time.perf_counter() - t0)
+    print("queries/s network", nn_rate, "MC", mc_rate)
+    assert nn_rate > 1000 * mc_rate
     # outside the trained distance range the MC kernel answers
     far = sg.training_pairs(4, 200_000, seed=13, d_min=100.0, d_max=120.0)
     out, used_mc = s.predict(far)
