@@ -861,7 +861,6 @@ def run_ours(args):
                      "traffic_note": "DRAM bytes per launch: ncu capture of a 2.5e8-photon launch scaled by photons",
                      "issue_active_ncu": roofline.NCU_ISSUE_ACTIVE,
                      "branch_efficiency_ncu": roofline.NCU_BRANCH_UNIFORM,
-                     "hit_writeback_gbs": hits_local / K * 64 / (reduce(t_local, MAX) / K) / 1e9,
                      "note": "issue-bound: ncu shows {:.0%} of issue slots busy (ALU pipe {:.0%}, FMA {:.0%}, XU {:.0%})".format(
                          roofline.NCU_ISSUE_ACTIVE, roofline.NCU_PIPES["alu"], roofline.NCU_PIPES["fma"],
                          roofline.NCU_PIPES["xu"]),
