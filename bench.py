@@ -276,6 +276,20 @@ def run_surrogate_workload(args):
                 acc[f"hits>={cut}"] = {"pairs": int(g.sum()), "median_rel_err": float(np.median(rel)),
                                        "frac_within_5pct": float(np.mean(rel < 0.05)),
                                        "sum_ratio": float(pred[g, 0].sum() / test.mu[g].sum())}
+        # the same held-out pairs with >= 1000 hits again at 1e7 photons (other seeds): a
+        # truth with 10x the statistics, and the 1e6-photon MC judged against it as the noise floor
+        g = test.hits >= 1000
+        hp = np.ascontiguousarray(test_pairs[g]).copy()
+        hp["n_photons"] = 10_000_000
+        hp["seed"] = [pp.propagation.pair_seed(args.seed + 77, i) for i in range(len(hp))]
+        hi = sg.mc_dataset(prop, hp, opts, min_hits_mu=0, min_hits_fit=0)
+        truth = hi.mu / 10.0
+        rel_nn = np.abs(pred[g, 0] - truth) / truth
+        rel_mc = np.abs(test.mu[g] - truth) / truth
+        acc["hits>=1000, 1e7-photon truth"] = {
+            "pairs": int(g.sum()), "median_rel_err": float(np.median(rel_nn)),
+            "frac_within_5pct": float(np.mean(rel_nn < 0.05)), "sum_ratio": float(pred[g, 0].sum() / truth.sum()),
+            "mc_1e6_median_rel_err": float(np.median(rel_mc)), "mc_1e6_frac_within_5pct": float(np.mean(rel_mc < 0.05))}
         r2 = {}
         for j, name in enumerate(["ln_mu_over_N", "logit_w", "ln_a1", "ln_a2", "ln_theta"]):
             m = test.mask[:, j] > 0
