@@ -814,16 +814,29 @@ pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, con
        (e = cudaMemsetAsync(d_mom, 0, rows * PP_FIT_MOMENTS * sizeof(double), s))))
     return c->cuda_fail(e, "pp_propagate_fit setup");
   // Waves of pairs whose hits fit the hit buffer: each wave propagates, then
-  // adds its hits' moments; the expected hits per pair are geometric, scaled
-  // by what the waves so far produced, and a wave that overflows is halved.
-  std::vector<double> est(n_pairs);
-  for (int64_t i = 0; i < n_pairs; ++i) est[i] = expected_hits_geo(pairs[i]);
+  // adds its hits' moments.  A pair's hits are estimated from geometry,
+  // scaled by what the waves so far produced; a wave that overflows still
+  // counted every pair's hits exactly (its statistics are complete and the
+  // photons are a fixed function of the seeds), so it is repacked with those
+  // counts and its reruns fit.
+  std::vector<double> geo(n_pairs), exact(n_pairs, -1.0);
+  for (int64_t i = 0; i < n_pairs; ++i) geo[i] = expected_hits_geo(pairs[i]);
   double scale = 4.0;
   int64_t total = 0;
+  std::vector<double> wst;
   for (int64_t start = 0; start < n_pairs;) {
-    int64_t end = start;
-    double acc = 0.0;
-    while (end < n_pairs && (end == start || acc + scale * est[end] <= 0.8 * (double)cap)) acc += scale * est[end++];
+    auto pick = [&](int64_t from) {
+      int64_t to = from;
+      double acc = 0.0;
+      while (to < n_pairs) {
+        const double w = exact[to] >= 0.0 ? exact[to] : scale * geo[to];
+        if (to > from && acc + w > 0.8 * (double)cap) break;
+        acc += w;
+        ++to;
+      }
+      return to;
+    };
+    int64_t end = pick(start);
     unsigned long long cnt[4];
     for (;;) {
       pp::LaunchArgs a = base_args(c, &o);
@@ -842,15 +855,23 @@ pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, con
           (e = cudaMemcpyAsync(cnt, c->counters.p, sizeof cnt, cudaMemcpyDeviceToHost, s)) ||
           (e = cudaStreamSynchronize(s)))
         return c->cuda_fail(e, "pp_propagate_fit wave");
-      double wave_est = 0.0;
-      for (int64_t i = start; i < end; ++i) wave_est += est[i];
-      if (wave_est > 0.0) scale = std::max(1.0, 1.25 * (double)cnt[0] / wave_est);
+      double wave_geo = 0.0;
+      bool all_geo = true;
+      for (int64_t i = start; i < end; ++i) {
+        wave_geo += geo[i];
+        all_geo = all_geo && exact[i] < 0.0;
+      }
+      if (all_geo && wave_geo > 0.0) scale = std::max(1.0, 1.25 * (double)cnt[0] / wave_geo);
       if (cnt[0] <= (unsigned long long)cap) break;
-      if (end - start == 1) {
-        *n_hits = (int64_t)cnt[0];
+      wst.resize((size_t)(end - start) * PP_STATS);
+      if ((e = cudaMemcpy(wst.data(), a.stats, wst.size() * sizeof(double), cudaMemcpyDeviceToHost)))
+        return c->cuda_fail(e, "pp_propagate_fit wave statistics");
+      for (int64_t i = start; i < end; ++i) exact[i] = wst[(size_t)(i - start) * PP_STATS];
+      if (exact[start] > (double)cap) {
+        *n_hits = (int64_t)exact[start];
         return c->fail(PP_ERR_OVERFLOW, "one pair has more hits than hit_capacity; raise hit_capacity");
       }
-      end = start + (end - start) / 2;
+      end = pick(start);
     }
     if ((e = pp::launch_fit_moments_hits(c->fitk, c->d_tables, d_pairs, n_pairs, o.mode,
                                          static_cast<const pp_hit*>(c->hits.p), (unsigned long long)cap,

@@ -132,7 +132,7 @@ def propagate_fit(propagator: Propagator, pairs, obs_angles, opts: RunOptions | 
     device (pp_propagate_fit).  hit_capacity sizes the device hit buffer
     (96 bytes per hit with the fit records); the library runs the pairs in
     waves that fit it.  The default is four times the geometric estimate of
-    the hits, between 2^16 and 2^25."""
+    the hits, between 2^16 and 2^25 (at most 3.2 GB of device memory)."""
     opts = opts or RunOptions(mode="compat", pmt_weight=True)
     o = opts.to_c()
     o.hist_bins = 0
