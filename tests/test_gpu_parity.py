@@ -377,3 +377,31 @@ def test_autotune_and_cache(propagator, tmp_path):
     assert again["block_size"] == best["block_size"] and again["chunk_photons"] == best["chunk_photons"]
     r = propagator.propagate(b, ro)
     assert r.n_hits > 0
+
+
+def test_full_size_benchmark_batch_properties(propagator):
+    """The 4096-pair benchmark batch at full size (5.75e9 photons), through
+    size-independent properties: batched and plain paths give the same hits
+    and statistics (the photons are a fixed function of the seeds), every
+    hit record agrees with its pair's FP64 sums, histograms hold the
+    in-window weight, and each pair counts all its photons."""
+    b = pp.batches.mixed_batch(4096, seed=2024)
+    ro = pp.RunOptions(mode="physical", g=0.95, t_max=1000.0, hist_bins=1000)
+    a = propagator.propagate(b, ro, hit_capacity=1 << 21)
+    c = propagator.propagate_plain(b, ro, hit_capacity=1 << 21)
+    assert not a.overflow and a.n_hits > 100_000
+    assert a.n_hits == c.n_hits
+    np.testing.assert_allclose(a.stats, c.stats, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(a.hist, c.hist, rtol=1e-9, atol=1e-15)
+    ha, hc = a.sorted_hits(), c.sorted_hits()
+    assert ha.tobytes() == hc.tobytes()
+    np.testing.assert_array_equal(a.stats[:, 6], b["n_photons"])
+    per_pair = np.bincount(ha["pair"], minlength=len(b))
+    np.testing.assert_array_equal(a.stats[:, 0], per_pair)
+    w = ha["weight"].astype(np.float64)
+    np.testing.assert_allclose(a.stats[:, 1], np.bincount(ha["pair"], weights=w, minlength=len(b)),
+                               rtol=1e-5, atol=1e-9)
+    t = ha["time"].astype(np.float64)
+    inwin = (t >= 0) & (t < 1000.0)
+    np.testing.assert_allclose(a.hist.sum(axis=1), np.bincount(ha["pair"][inwin], weights=w[inwin],
+                                                               minlength=len(b)), rtol=1e-5, atol=1e-9)
