@@ -242,6 +242,44 @@ def surrogate_inference_rate(device, n=1_000_000, net=None, reps=10):
     return {"queries": n, "seconds_per_batch": t, "queries_per_s": n / t, "tflops": flops / t / 1e12}
 
 
+def arrival_time_shape(test, g, pred, hi, opts):
+    """How well the predicted arrival-time mixture matches the MC's residual
+    time distribution on the selected held-out pairs: the Kolmogorov distance
+    between the mixture's CDF and the 1e7-photon MC histogram's CDF, beside
+    that of the pair's own EM fit (what a 2-Gamma mixture can do) and of the
+    1e6-photon MC histogram (the noise floor), and the error of the mean."""
+    from scipy import stats
+    t0, bw, bins = opts.hist_t0, opts.hist_bin_width, opts.hist_bins
+    edges = t0 + bw * np.arange(1, bins + 1)
+
+    def mix_cdf(p, r):
+        w, a1, a2, th = p
+        return w * stats.gamma.cdf(r, a1, scale=th) + (1 - w) * stats.gamma.cdf(r, a2, scale=th)
+
+    ks_nn, ks_fit, ks_mc, mean_err = [], [], [], []
+    fits = test.y[g].astype(np.float64)
+    for i, k in enumerate(np.nonzero(g)[0]):
+        h_hi = hi.hist[i]
+        if h_hi.sum() <= 0:
+            continue
+        r = edges - test.tshift[k]
+        c_hi = np.cumsum(h_hi) / h_hi.sum()
+        c_lo = np.cumsum(test.hist[k]) / max(test.hist[k].sum(), 1e-300)
+        w_fit = 1 / (1 + np.exp(-fits[i, 1]))
+        ks_nn.append(np.max(np.abs(mix_cdf(pred[k, 1:5], r) - c_hi)))
+        ks_fit.append(np.max(np.abs(mix_cdf((w_fit, *np.exp(fits[i, 2:5])), r) - c_hi)))
+        ks_mc.append(np.max(np.abs(c_lo - c_hi)))
+        centres = edges - 0.5 * bw - test.tshift[k]
+        m_hi = float(np.sum(h_hi * centres) / h_hi.sum())
+        w, a1, a2, th = pred[k, 1:5]
+        m_nn = th * (w * a1 + (1 - w) * a2)
+        mean_err.append(abs(m_nn - m_hi) / max(abs(m_hi), 1e-9))
+    return {"pairs": len(ks_nn), "median_ks_surrogate": float(np.median(ks_nn)),
+            "median_ks_em_fit": float(np.median(ks_fit)), "median_ks_mc_1e6": float(np.median(ks_mc)),
+            "median_rel_err_mean_residual": float(np.median(mean_err)),
+            "what": "Kolmogorov distance to the 1e7-photon MC residual-time CDF"}
+
+
 def run_surrogate_workload(args):
     """--workload surrogate: MC training set (mixed-batch geometry, 1e6 photons
     per pair), training by the library's kernels, held-out accuracy against MC,
@@ -260,7 +298,7 @@ def run_surrogate_workload(args):
                                                       distance_law=args.train_distance), opts,
                               full_weight_hits=args.full_weight_hits)
         test_pairs = sg.training_pairs(args.test_pairs, 1_000_000, seed=args.seed + 1)
-        test = sg.mc_dataset(prop, test_pairs, opts)
+        test = sg.mc_dataset(prop, test_pairs, opts, return_hist=True)
         t_data = time.perf_counter() - t0
         s = sg.Surrogate(prop, opts, seed=args.seed)
         t0 = time.perf_counter()
@@ -282,7 +320,7 @@ def run_surrogate_workload(args):
         hp = np.ascontiguousarray(test_pairs[g]).copy()
         hp["n_photons"] = 10_000_000
         hp["seed"] = [pp.propagation.pair_seed(args.seed + 77, i) for i in range(len(hp))]
-        hi = sg.mc_dataset(prop, hp, opts, min_hits_mu=0, min_hits_fit=0)
+        hi = sg.mc_dataset(prop, hp, opts, min_hits_mu=0, min_hits_fit=0, return_hist=True)
         truth = hi.mu / 10.0
         rel_nn = np.abs(pred[g, 0] - truth) / truth
         rel_mc = np.abs(test.mu[g] - truth) / truth
@@ -290,6 +328,7 @@ def run_surrogate_workload(args):
             "pairs": int(g.sum()), "median_rel_err": float(np.median(rel_nn)),
             "frac_within_5pct": float(np.mean(rel_nn < 0.05)), "sum_ratio": float(pred[g, 0].sum() / truth.sum()),
             "mc_1e6_median_rel_err": float(np.median(rel_mc)), "mc_1e6_frac_within_5pct": float(np.mean(rel_mc < 0.05))}
+        acc["arrival_time_shape, hits>=1000"] = arrival_time_shape(test, g, pred, hi, opts)
         r2 = {}
         for j, name in enumerate(["ln_mu_over_N", "logit_w", "ln_a1", "ln_a2", "ln_theta"]):
             m = test.mask[:, j] > 0

@@ -131,20 +131,24 @@ class Dataset:
     hits: np.ndarray   # [n] detected photons (unweighted)
     mu: np.ndarray     # [n] sum of weights
     sigma_mu: np.ndarray  # [n] statistical error of mu: sqrt(sum of squared weights)
+    hist: np.ndarray | None = None    # [n, bins] arrival-time histograms (return_hist=True)
+    tshift: np.ndarray | None = None  # [n] t_geo of each pair (ns)
 
     def subset(self, idx):
-        return Dataset(self.x[idx], self.y[idx], self.mask[idx], self.hits[idx], self.mu[idx], self.sigma_mu[idx])
+        return Dataset(self.x[idx], self.y[idx], self.mask[idx], self.hits[idx], self.mu[idx], self.sigma_mu[idx],
+                       None if self.hist is None else self.hist[idx],
+                       None if self.tshift is None else self.tshift[idx])
 
 
 def mc_dataset(prop: Propagator, pairs, opts: RunOptions, min_hits_mu=1, min_hits_fit=1000, chunk=20000,
-               fit_iters=60, full_weight_hits=100.0) -> Dataset:
+               fit_iters=60, full_weight_hits=100.0, return_hist=False) -> Dataset:
     """Propagates the pairs (MC kernel, histograms only) and turns their
     statistics and histograms into targets."""
     import torch
     dev = torch.device("cuda", prop.device)
     c = opts.to_c()
     bins = c.hist_bins
-    cols = {k: [] for k in ("x", "y", "m", "h", "mu", "sg")}
+    cols = {k: [] for k in ("x", "y", "m", "h", "mu", "sg", "hist", "ts")}
     o = RunOptions(**{**opts.__dict__})
     o.write_hits = False
     for s0 in range(0, len(pairs), chunk):
@@ -186,7 +190,14 @@ def mc_dataset(prop: Propagator, pairs, opts: RunOptions, min_hits_mu=1, min_hit
         cols["h"].append(nh)
         cols["mu"].append(mu)
         cols["sg"].append(np.sqrt(st[:, 2]))
-    return Dataset(*(np.concatenate(cols[k]) for k in ("x", "y", "m", "h", "mu", "sg")))
+        if return_hist:
+            cols["hist"].append(d_hist.cpu().numpy())
+            cols["ts"].append(d_ts.cpu().numpy())
+    ds = Dataset(*(np.concatenate(cols[k]) for k in ("x", "y", "m", "h", "mu", "sg")))
+    if return_hist:
+        ds.hist = np.concatenate(cols["hist"])
+        ds.tshift = np.concatenate(cols["ts"])
+    return ds
 
 
 def training_pairs(n_pairs, photons, seed=0, d_min=2.0, d_max=150.0, distance_law="uniform"):
