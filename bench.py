@@ -876,6 +876,39 @@ def run_ours(args):
                  "launches_per_pass": 3 * n_pairs}
         plain["batched_over_plain_kernel"] = value / plain["kernel_photons_per_s"]
         plain["batched_over_plain_host_api"] = value / plain["host_api_photons_per_s"]
+        # the reference's own launch shape: cuda_propagate_photons! as propagate_distance launches
+        # it (16 blocks x 1024 threads, per-block hit stacks), one pair per launch, on the first
+        # 256 pairs of the same batch
+        nref, blocks, threads, stack_len = min(256, n_pairs), 16, 1024, 65536
+        arrs = pp.initialize_photon_arrays(stack_len, blocks, device=dev)
+
+        def ref_pass():
+            for i in range(nref):
+                prop.cuda_propagate_photons(*arrs, stack_len, h_pairs[i], ro, threads, stream=s)
+        ref_pass()
+        s.synchronize()
+        e0.record(s)
+        ref_pass()
+        e1.record(s)
+        s.synchronize()
+        t_ref = e0.elapsed_time(e1) / 1e3
+        # every thread simulates cld(N, blocks x threads) photons, so a launch simulates that many
+        # rounds of 16384 photons unless a block's stack fills first (checked on a sample)
+        per = blocks * threads
+        sim = -(-np.asarray(b["n_photons"][:nref], dtype=np.int64) // per) * per
+        full = True
+        for i in range(0, nref, 17):
+            with torch.cuda.stream(s):
+                arrs[5].zero_()  # the kernel adds to the count, like the reference's atomic_add!
+            prop.cuda_propagate_photons(*arrs, stack_len, h_pairs[i], ro, threads, stream=s)
+            s.synchronize()
+            full = full and int(arrs[5][0].item()) == int(sim[i])
+        ph_ref = float(sim.sum())
+        plain["reference_launch_shape"] = {
+            "photons_per_s": ph_ref / t_ref, "pairs": nref, "photons": ph_ref, "all_photons_simulated": full,
+            "what": "pp_cuda_propagate_photons per pair, 16 x 1024 threads as propagate_distance launches "
+                    "cuda_propagate_photons! (src/photon_prop_cuda.jl:598-606), synchronous per call as there"}
+        plain["batched_over_reference_launch_shape"] = value / (ph_ref / t_ref)
 
     # e2e: the C-ABI host-buffer call, pinned host memory, copies inside the timing
     pin_pairs = [torch.from_numpy(b.view(np.uint8).copy()).pin_memory().numpy().view(pp.PAIR_DTYPE)
