@@ -47,13 +47,23 @@ typedef enum {
 } pp_status;
 
 enum { PP_MODE_COMPAT = 0, PP_MODE_PHYSICAL = 1 };
-enum { PP_EMITTER_ISOTROPIC = 0, PP_EMITTER_CHERENKOV_CONE = 1 };
+/* PP_EMITTER_CASCADE: a point source with the angular profile of an EM
+ * cascade about `dir`, cherenkov_ang_dist(cos theta, n(lambda))
+ * (src/emission.jl:32-44), sampled by inverse CDF; physical mode only (the
+ * reference propagates isotropic photons and reweights them to this profile,
+ * src/modelling.jl:46-49). */
+enum { PP_EMITTER_ISOTROPIC = 0, PP_EMITTER_CHERENKOV_CONE = 1, PP_EMITTER_CASCADE = 2 };
 enum { PP_SPECTRUM_CHERENKOV = 0, PP_SPECTRUM_MONOCHROMATIC = 1 };
 enum {
   PP_OPT_PMT_WEIGHT = 1u, /* multiply hit weights by the PMT acceptance */
   PP_OPT_NORMALIZE = 2u,  /* divide each pair's histogram by its photon count */
   PP_OPT_NO_HITS = 4u,    /* accumulate statistics only; write no hit records */
-  PP_OPT_COMPACT_HITS = 8u /* write pp_hit32 records instead of pp_hit */
+  PP_OPT_COMPACT_HITS = 8u, /* write pp_hit32 records instead of pp_hit */
+  PP_OPT_CASCADE = 16u      /* the pairs may include PP_EMITTER_CASCADE: launch the kernel variant that
+                               samples the cascade profile.  The host-buffer entry points set it
+                               themselves; on the *_device entry points the caller sets it, and a
+                               cascade pair launched without it is emitted on the Cherenkov cone
+                               and sets status bit 4 (value 4) in counters[2]. */
 };
 
 #define PP_MAX_KNOTS 64
@@ -294,6 +304,10 @@ PP_API double pp_cherenkov_ang_dist_int_exact(double ref_index, double lower, do
 /* cherenkov_ang_dist_int: linear interpolation of the [-1, 1] integral on
  * ref_index = 1.1:0.01:1.5, src/emission.jl:88-99 (NaN outside). */
 PP_API double pp_cherenkov_ang_dist_int(double ref_index);
+/* cos(theta) of the cascade emitter for a uniform u in (0, 1) at refractive
+ * index n, from the library's FP64 tables (the kernel samples the same
+ * tables in FP32). */
+PP_API double pp_cascade_cos_theta(double u, double ref_index);
 /* get_dir_reweight(thetas, obs_angle, ref_ixs), src/modelling.jl:46-49:
  * out[i] = cherenkov_ang_dist(cos(thetas[i] - obs_angle), ref_ixs[i]) /
  *          (2 cherenkov_ang_dist_int(ref_ixs[i])). */
@@ -381,8 +395,9 @@ PP_API pp_status pp_fractional_contrib_long(const pp_medium_desc* m, int32_t ly_
  * cherenkov_track_length(E) x fractional share) photons, written as pairs
  * (position, time, direction, photons, `emitter`; target and seed unset):
  * source k of particle p is d_sources[p * (n_grid - 1) + k].  An isotropic
- * source sits at the midpoint; a Cherenkov-cone source is a track over its
- * interval along the particle.  n_grid comes back in *n_grid. */
+ * or cascade-profile source sits at the midpoint; a Cherenkov-cone source is
+ * a track over its interval along the particle.  n_grid comes back in
+ * *n_grid. */
 PP_API pp_status pp_particles_to_sources_device(pp_ctx* ctx, const pp_particle* d_particles, int64_t n_particles,
                                                 double len_min, double len_max, double precision, int32_t ly_mode,
                                                 double wl_min, double wl_max, int32_t emitter, pp_pair* d_sources,
@@ -518,7 +533,7 @@ PP_API pp_status pp_autotune(pp_ctx* ctx, const pp_pair* pairs, int64_t n_pairs,
  * 4 update_position (in: pos[3],dir[3],step; out: 3), 5 equidistant
  * interpolation of the context's knots (in: u), 6 refractive index,
  * 7 group index, 8 scattering length, 9 absorption length, 10 PMT
- * acceptance (in: wavelength). */
+ * acceptance (in: wavelength), 11 cascade-emitter cos theta (in: u, n). */
 PP_API pp_status pp_device_eval(pp_ctx* ctx, int32_t op, const double* in, double* out, int64_t n);
 
 /* Measures this device's FP32 FMA and MUFU (transcendental) issue peaks with

@@ -134,3 +134,55 @@ def fit_photon_dist(obs_angles, tres, thetas, ref_ix, abs_weight, pmt_weight, n_
         rows.append((a, al, th, m[0] / n_ph_gen))
         mom.append(m)
     return np.array(rows), np.array(mom)
+
+
+# ---- cascade emitter: inverse-CDF sampling of the angular profile --------
+CASC_NF, CASC_NI, CASC_VMIN, CASC_VMAX = 2048, 8192, -1.85, 0.35
+_CASC = None
+
+
+def cascade_G(v):
+    """Antiderivative of a exp(b |v|^c) + d: sign(v) (a/c) k^(-1/c) gamma(1/c, k |v|^c) + d v
+    (k = -b; scipy's regularised lower incomplete gamma times Gamma(1/c))."""
+    v = np.asarray(v, dtype=np.float64)
+    k, s = -B, 1.0 / C
+    p = (A / C) * k ** (-s) * special.gammainc(s, k * np.abs(v) ** C) * special.gamma(s)
+    return np.sign(v) * p + D * v
+
+
+def cascade_tables():
+    """(forward G table, inverse v table, vmin, dv, gmin, dg), FP64."""
+    global _CASC
+    if _CASC is None:
+        v = CASC_VMIN + (CASC_VMAX - CASC_VMIN) / CASC_NF * np.arange(CASC_NF + 1)
+        fwd = cascade_G(v)
+        levels = fwd[0] + (fwd[-1] - fwd[0]) * np.arange(CASC_NI + 1) / CASC_NI
+        lo = np.full_like(levels, CASC_VMIN)
+        hi = np.full_like(levels, CASC_VMAX)
+        for _ in range(64):
+            mid = 0.5 * (lo + hi)
+            below = cascade_G(mid) < levels
+            lo = np.where(below, mid, lo)
+            hi = np.where(below, hi, mid)
+        inv = 0.5 * (lo + hi)
+        inv[0], inv[-1] = CASC_VMIN, CASC_VMAX
+        _CASC = (np.ascontiguousarray(fwd), np.ascontiguousarray(inv), CASC_VMIN,
+                 (CASC_VMAX - CASC_VMIN) / CASC_NF, float(fwd[0]), float(fwd[-1] - fwd[0]) / CASC_NI)
+    return _CASC
+
+
+def cascade_cos_theta(u, n):
+    """cos(theta) sampled from the profile at refractive index n for uniform u."""
+    fwd, inv, vmin, dv, gmin, dg = cascade_tables()
+
+    def lerp(t, x):
+        cells = len(t) - 1
+        x = np.clip(x, 0.0, cells)
+        i = np.minimum(np.floor(x).astype(np.int64), cells - 1)
+        return t[i] + (x - i) * (t[i + 1] - t[i])
+    c0 = 1.0 / np.asarray(n, dtype=np.float64)
+    gl = lerp(fwd, (-1.0 - c0 - vmin) / dv)
+    gh = lerp(fwd, (1.0 - c0 - vmin) / dv)
+    v = lerp(inv, (gl + np.asarray(u, dtype=np.float64) * (gh - gl) - gmin) / dg)
+    return np.clip(v + c0, -1.0, 1.0)
+

@@ -41,7 +41,10 @@ class Tables(ctypes.Structure):
         ("pad", ctypes.c_int32),
         ("knots", ctypes.c_double * MAX_KNOTS),
         ("abs_wl", ctypes.c_double * MAX_ABS), ("abs_len", ctypes.c_double * MAX_ABS),
-        ("pmt_wl", ctypes.c_double * MAX_PMT), ("pmt_acc", ctypes.c_double * MAX_PMT)]
+        ("pmt_wl", ctypes.c_double * MAX_PMT), ("pmt_acc", ctypes.c_double * MAX_PMT),
+        ("casc_fwd", ctypes.c_void_p), ("casc_inv", ctypes.c_void_p),
+        ("casc_vmin", ctypes.c_double), ("casc_dv", ctypes.c_double), ("casc_gmin", ctypes.c_double),
+        ("casc_dg", ctypes.c_double), ("casc_nf", ctypes.c_int32), ("casc_ni", ctypes.c_int32)]
 
 
 class Opts(ctypes.Structure):
@@ -161,6 +164,12 @@ def make_tables(medium: tb.Water, knots, pmt=None, abs_table=None) -> Tables:
     t.n_pmt = len(pmt[0])
     t.pmt_wl[:len(pmt[0])] = list(pmt[0])
     t.pmt_acc[:len(pmt[1])] = list(pmt[1])
+    from . import fits
+    fwd, inv, vmin, dv, gmin, dg = fits.cascade_tables()
+    t._casc = (fwd, inv)  # keeps the arrays alive with the struct
+    t.casc_fwd, t.casc_inv = fwd.ctypes.data, inv.ctypes.data
+    t.casc_vmin, t.casc_dv, t.casc_gmin, t.casc_dg = vmin, dv, gmin, dg
+    t.casc_nf, t.casc_ni = len(fwd) - 1, len(inv) - 1
     return t
 
 

@@ -168,6 +168,25 @@ static void philox_block(uint64_t seed, int64_t photon, uint32_t block, double u
   for (int i = 0; i < 4; ++i) u[i] = orc_uniform(w[i]);
 }
 
+/* cos(theta) of the cascade emitter: inverse CDF of the EM-cascade profile
+ * cherenkov_ang_dist (src/emission.jl:32-44) at 1/n = c0 through the
+ * tables (linear interpolation). */
+static double lerp_tab(const double* t, int cells, double x) {
+  if (x < 0.0) x = 0.0;
+  if (x > cells) x = cells;
+  int i = (int)x;
+  if (i > cells - 1) i = cells - 1;
+  return t[i] + (x - i) * (t[i + 1] - t[i]);
+}
+
+static double cascade_cos_theta(const orc_tables* T, double c0, double u) {
+  const double gl = lerp_tab(T->casc_fwd, T->casc_nf, (-1.0 - c0 - T->casc_vmin) / T->casc_dv);
+  const double gh = lerp_tab(T->casc_fwd, T->casc_nf, (1.0 - c0 - T->casc_vmin) / T->casc_dv);
+  const double v = lerp_tab(T->casc_inv, T->casc_ni, (gl + u * (gh - gl) - T->casc_gmin) / T->casc_dg);
+  const double x = v + c0;
+  return x < -1.0 ? -1.0 : (x > 1.0 ? 1.0 : x);
+}
+
 /* One photon: the per-photon body of cuda_propagate_photons!,
  * src/photon_prop_cuda.jl:301-380, plus the host finish of
  * propagate_distance (:622, :634-638) done per hit. */
@@ -197,6 +216,12 @@ static int simulate_photon(const orc_tables* T, const orc_pair* P, int64_t pair_
     pos[0] = P->pos[0];
     pos[1] = P->pos[1];
     pos[2] = P->pos[2];
+  } else if (P->emitter == 2) {
+    double ct = cascade_cos_theta(T, 1.0 / orc_refractive_index(T, wl), u[1]);
+    double st = sqrt(fmax(0.0, fma(-ct, ct, 1.0)));
+    double loc[3] = {cp * st, sp * st, ct};
+    orc_rotate_to_axis(P->dir, loc, dir);
+    for (int j = 0; j < 3; ++j) pos[j] = P->pos[j];
   } else {
     double ct = 1.0 / orc_refractive_index(T, wl);
     double st = sqrt(fmax(0.0, fma(-ct, ct, 1.0)));

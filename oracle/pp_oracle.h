@@ -31,6 +31,13 @@ typedef struct {
   double knots[ORC_MAX_KNOTS];
   double abs_wl[ORC_MAX_ABS], abs_len[ORC_MAX_ABS];
   double pmt_wl[ORC_MAX_PMT], pmt_acc[ORC_MAX_PMT];
+  /* cascade emitter (emitter 2): G of the angular profile on casc_nf + 1
+   * points from casc_vmin, step casc_dv; v at casc_ni + 1 levels of G from
+   * casc_gmin, step casc_dg (NULL: no cascade emitter) */
+  const double* casc_fwd;
+  const double* casc_inv;
+  double casc_vmin, casc_dv, casc_gmin, casc_dg;
+  int32_t casc_nf, casc_ni;
 } orc_tables;
 
 typedef struct {
@@ -42,7 +49,7 @@ typedef struct {
   double radius;
   int64_t n_photons;
   uint64_t seed;
-  int32_t emitter; /* 0 isotropic point, 1 Cherenkov-cone line */
+  int32_t emitter; /* 0 isotropic point, 1 Cherenkov-cone line, 2 cascade-profile point */
   int32_t pad;
 } orc_pair;
 

@@ -104,6 +104,7 @@ struct pp_ctx {
   std::string err;
   std::vector<unsigned char> h_tables;
   void* d_tables = nullptr;
+  void* d_casc = nullptr;  // cascade emitter tables (float)
   cudaStream_t stream = nullptr;
   // buffers of the host-buffer entry points
   DevBuf pairs, hits, counters, stats, hist;
@@ -169,17 +170,18 @@ pp_status validate_pairs(pp_ctx* c, const pp_pair* p, int64_t n, int mode) {
       snprintf(buf, sizeof buf, "pair %lld: radius must be > 0", (long long)i);
       return c->fail(PP_ERR_ARG, buf);
     }
-    if (q.emitter == PP_EMITTER_CHERENKOV_CONE) {
+    if (q.emitter == PP_EMITTER_CHERENKOV_CONE || q.emitter == PP_EMITTER_CASCADE) {
       if (mode == PP_MODE_COMPAT) {
         snprintf(buf, sizeof buf,
-                 "pair %lld: Cherenkov-cone emission has no reference-compatible form "
+                 "pair %lld: %s emission has no reference-compatible form "
                  "(the reference's initialize_direction throws ArgumentError)",
-                 (long long)i);
+                 (long long)i, q.emitter == PP_EMITTER_CASCADE ? "cascade" : "Cherenkov-cone");
         return c->fail(PP_ERR_ARG, buf);
       }
       const float n2 = q.dir[0] * q.dir[0] + q.dir[1] * q.dir[1] + q.dir[2] * q.dir[2];
       if (!(std::fabs(n2 - 1.f) < 1e-3f) || !(q.track_len >= 0.f)) {
-        snprintf(buf, sizeof buf, "pair %lld: cone emitter needs a unit direction and track_len >= 0", (long long)i);
+        snprintf(buf, sizeof buf, "pair %lld: cone and cascade emitters need a unit direction and track_len >= 0",
+                 (long long)i);
         return c->fail(PP_ERR_ARG, buf);
       }
     } else if (q.emitter != PP_EMITTER_ISOTROPIC) {
@@ -188,6 +190,12 @@ pp_status validate_pairs(pp_ctx* c, const pp_pair* p, int64_t n, int mode) {
     }
   }
   return PP_OK;
+}
+
+bool any_cascade(const pp_pair* p, int64_t n) {
+  for (int64_t i = 0; i < n; ++i)
+    if (p[i].emitter == PP_EMITTER_CASCADE) return true;
+  return false;
 }
 
 void resolve_launch(pp_ctx* c, const pp_run_opts& o, int& grid, int& block, uint32_t& chunk) {
@@ -420,12 +428,28 @@ pp_status pp_create(pp_ctx** out, int device, const pp_medium_desc* medium, cons
   pp::fill_fit_consts(&c->fitk, pp_refractive_index(medium, 800.0), pp_group_index(medium, 800.0));
   c->h_tables.resize(pp::dev_tables_size());
   pp::fill_dev_tables(c->h_tables.data(), coeffs, fk, n_knots, aw, al, n_abs, pw.data(), pa.data(), n_pmt);
+  {
+    std::vector<double> fwd(pp::kCascNF + 1), inv(pp::kCascNI + 1);
+    pp::cascade_tables(fwd.data(), inv.data());
+    std::vector<float> ft(fwd.begin(), fwd.end());
+    ft.insert(ft.end(), inv.begin(), inv.end());
+    if ((e = cudaMalloc(&c->d_casc, ft.size() * sizeof(float))) ||
+        (e = cudaMemcpy(c->d_casc, ft.data(), ft.size() * sizeof(float), cudaMemcpyHostToDevice))) {
+      g_create_error = std::string("pp_create: ") + cudaGetErrorString(e);
+      cudaGetLastError();
+      if (c->d_casc) cudaFree(c->d_casc);
+      delete c;
+      return e == cudaErrorMemoryAllocation ? PP_ERR_OOM : PP_ERR_CUDA;
+    }
+    pp::set_cascade_tables(c->h_tables.data(), static_cast<const float*>(c->d_casc), fwd.front(), fwd.back());
+  }
   if ((e = cudaMalloc(&c->d_tables, c->h_tables.size())) ||
       (e = cudaMemcpy(c->d_tables, c->h_tables.data(), c->h_tables.size(), cudaMemcpyHostToDevice)) ||
       (e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking))) {
     g_create_error = std::string("pp_create: ") + cudaGetErrorString(e);
     cudaGetLastError();
     if (c->d_tables) cudaFree(c->d_tables);
+    cudaFree(c->d_casc);
     delete c;
     return e == cudaErrorMemoryAllocation ? PP_ERR_OOM : PP_ERR_CUDA;
   }
@@ -444,6 +468,7 @@ void pp_destroy(pp_ctx* c) {
                       &c->fit_rec, &c->fit_moments, &c->fit_out, &c->fit_cs})
       b->release();
     if (c->d_tables) cudaFree(c->d_tables);
+    if (c->d_casc) cudaFree(c->d_casc);
     if (c->stream) cudaStreamDestroy(c->stream);
   }
   delete c;
@@ -507,6 +532,9 @@ pp_status pp_propagate(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const p
   if ((st = validate_pairs(c, pairs, n_pairs, opts->mode))) return st;
   if (cap < 0 || (cap > 0 && !hits) || !n_hits || !stats || (opts->hist_bins > 0 && !hist))
     return c->fail(PP_ERR_ARG, "pp_propagate: bad buffer arguments");
+  pp_run_opts o_local = *opts;
+  if (any_cascade(pairs, n_pairs)) o_local.flags |= PP_OPT_CASCADE;
+  opts = &o_local;
   DeviceGuard guard(c->device);
   const int bins = opts->hist_bins;
   cudaError_t e;
@@ -569,6 +597,9 @@ pp_status pp_propagate_plain_device(pp_ctx* c, const pp_pair* d_pair, const pp_p
       !aligned(d_hist, 8))
     return c->fail(PP_ERR_ARG, "pp_propagate_plain_device: pair/hits need 16-byte, counters/stats/hist 8-byte alignment");
   if ((st = validate_pairs(c, h_pair, 1, opts->mode))) return st;
+  pp_run_opts o_local = *opts;
+  if (any_cascade(h_pair, 1)) o_local.flags |= PP_OPT_CASCADE;
+  opts = &o_local;
   DeviceGuard guard(c->device);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   pp::LaunchArgs a = base_args(c, opts);
@@ -599,6 +630,7 @@ pp_status pp_propagate_plain_device(pp_ctx* c, const pp_pair* d_pair, const pp_p
 pp_status pp_propagate_plain(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp_run_opts* opts,
                              pp_hit* hits, int64_t cap, int64_t* n_hits, double* stats, double* hist) {
   if (!c) return PP_ERR_ARG;
+  pp_run_opts o_plain;
   {
     std::lock_guard<std::mutex> lk(c->mu);
     pp_status st = validate_opts(c, opts);
@@ -606,6 +638,11 @@ pp_status pp_propagate_plain(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, c
     if ((st = validate_pairs(c, pairs, n_pairs, opts->mode))) return st;
     if (cap < 0 || (cap > 0 && !hits) || !n_hits || !stats || (opts->hist_bins > 0 && !hist))
       return c->fail(PP_ERR_ARG, "pp_propagate_plain: bad buffer arguments");
+    if (any_cascade(pairs, n_pairs) && !(opts->flags & PP_OPT_CASCADE)) {
+      o_plain = *opts;
+      o_plain.flags |= PP_OPT_CASCADE;
+      opts = &o_plain;
+    }
     DeviceGuard guard(c->device);
     const int bins = opts->hist_bins;
     cudaError_t e;
@@ -699,9 +736,9 @@ pp_status pp_cuda_propagate_photons(pp_ctx* c, float* pos, float* dir, float* wl
 pp_status pp_device_eval(pp_ctx* c, int32_t op, const double* in, double* out, int64_t n) {
   if (!c) return PP_ERR_ARG;
   std::lock_guard<std::mutex> lk(c->mu);
-  static const int in_w[] = {6, 1, 2, 6, 7, 1, 1, 1, 1, 1, 1};
-  static const int out_w[] = {4, 1, 1, 3, 3, 1, 1, 1, 1, 1, 1};
-  if (op < 0 || op > 10 || n < 0 || (n > 0 && (!in || !out))) return c->fail(PP_ERR_ARG, "pp_device_eval: bad arguments");
+  static const int in_w[] = {6, 1, 2, 6, 7, 1, 1, 1, 1, 1, 1, 2};
+  static const int out_w[] = {4, 1, 1, 3, 3, 1, 1, 1, 1, 1, 1, 1};
+  if (op < 0 || op > 11 || n < 0 || (n > 0 && (!in || !out))) return c->fail(PP_ERR_ARG, "pp_device_eval: bad arguments");
   if (n == 0) return PP_OK;
   DeviceGuard guard(c->device);
   double *din = nullptr, *dout = nullptr;
@@ -787,6 +824,7 @@ pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, con
     return c->fail(PP_ERR_ARG, "need 1 <= n_angles <= PP_MAX_FIT_ANGLES observation angles");
   pp_run_opts o = *opts;
   o.flags &= ~(uint32_t)(PP_OPT_NO_HITS | PP_OPT_COMPACT_HITS);  // the fit reads full hit records
+  if (any_cascade(pairs, n_pairs)) o.flags |= PP_OPT_CASCADE;
   if (!hist) o.hist_bins = 0;
   const int bins = o.hist_bins;
   DeviceGuard guard(c->device);
@@ -963,6 +1001,9 @@ pp_status pp_autotune(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp
     if ((st = validate_opts(c, opts))) return st;
     if ((st = validate_pairs(c, pairs, n_pairs, opts->mode))) return st;
   }
+  pp_run_opts o_tune = *opts;
+  if (any_cascade(pairs, n_pairs)) o_tune.flags |= PP_OPT_CASCADE;
+  opts = &o_tune;
   const int m = opts->mode;
   if (cache_path) {
     std::ifstream f(cache_path);

@@ -129,6 +129,10 @@ struct DevTables {
   float abs_len[PP_MAX_ABS];
   float pmt_wl[PP_MAX_PMT];
   float pmt_acc[PP_MAX_PMT];
+  // cascade emitter: device tables (forward G, then inverse v) and their grids
+  const float* casc;
+  float casc_vmin, casc_inv_dv, casc_gmin, casc_inv_dg;
+  int32_t casc_nf, casc_ni;
 };
 static_assert(sizeof(DevTables) % 16 == 0, "DevTables is copied as 16-byte words");
 
@@ -173,6 +177,22 @@ __device__ __forceinline__ float draw_wavelength(const DevTables& T, float u) {
   i = min(i, T.n_knots - 2);
   const float f = x - (float)i;
   return fmaf(T.knots[i + 1] - T.knots[i], f, T.knots[i]);
+}
+
+// cos(theta) of the cascade emitter: inverse-CDF sample of
+// a exp(b |x - c0|^c) + d on [-1, 1], c0 = 1/n (cherenkov_ang_dist,
+// src/emission.jl:32-44), from the tables of G(v) = integral of the profile.
+__device__ __forceinline__ float casc_lerp(const float* __restrict__ t, int cells, float x) {
+  x = fminf(fmaxf(x, 0.f), (float)cells);
+  const int i = min((int)x, cells - 1);
+  const float a = __ldg(t + i), b = __ldg(t + i + 1);
+  return fmaf(x - (float)i, b - a, a);
+}
+__device__ __forceinline__ float cascade_cos_theta(const DevTables& T, float c0, float u) {
+  const float gl = casc_lerp(T.casc, T.casc_nf, (-1.f - c0 - T.casc_vmin) * T.casc_inv_dv);
+  const float gh = casc_lerp(T.casc, T.casc_nf, (1.f - c0 - T.casc_vmin) * T.casc_inv_dv);
+  const float v = casc_lerp(T.casc + T.casc_nf + 1, T.casc_ni, (fmaf(u, gh - gl, gl) - T.casc_gmin) * T.casc_inv_dg);
+  return fminf(fmaxf(v + c0, -1.f), 1.f);
 }
 
 // cos(theta) of Henyey-Greenstein scattering (src/photon_prop_cuda.jl:31-38)
@@ -285,7 +305,13 @@ struct EmissionFrame {
   bool axis_ez;  // isotropic: the axis is e_z
 };
 
-template <int MODE>
+// EM selects the emitters a kernel variant samples: 0 isotropic and cone
+// (a cascade pair is then emitted on the cone; the batched kernel flags it),
+// kEmCascade also the cascade profile, whose table lookups would otherwise
+// cost every variant registers.
+enum { kEmBasic = 0, kEmCascade = 1 };
+
+template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ EmissionFrame emission_frame(const DevTables& T, const pp_pair* __restrict__ P,
                                                         const Draw4& d) {
   const float4 pt = __ldg(reinterpret_cast<const float4*>(P));      // pos, t0
@@ -312,12 +338,14 @@ __device__ __forceinline__ EmissionFrame emission_frame(const DevTables& T, cons
     } else {
       f.cpol = fmaf(2.f, d.u1, -1.f);
     }
-  } else {
+  } else {  // Cherenkov cone (a track), or the cascade profile (a point)
     f.ox = dl.x;
     f.oy = dl.y;
     f.oz = dl.z;
-    f.cpol = rcp(phase_index(T, rcp(f.wl)));
-    const float s = d.u1 * dl.w;
+    const float c0 = rcp(phase_index(T, rcp(f.wl)));
+    const bool casc = EM == kEmCascade && emitter == PP_EMITTER_CASCADE;
+    f.cpol = casc ? cascade_cos_theta(T, c0, d.u1) : c0;
+    const float s = casc ? 0.f : d.u1 * dl.w;
     f.px = fmaf(s, f.ox, f.px);
     f.py = fmaf(s, f.oy, f.py);
     f.pz = fmaf(s, f.oz, f.pz);
@@ -355,11 +383,11 @@ __device__ __forceinline__ void emission_direction(const EmissionFrame& f, float
 
 // Emission of photon s.id (block 0): position, direction and the
 // per-wavelength constants; afterwards the next event is block 1.
-template <int MODE>
+template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                            const PairCtx& c, Photon& s) {
   const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, ctr_word(s.id, 0u));
-  const EmissionFrame f = emission_frame<MODE>(T, P, d);
+  const EmissionFrame f = emission_frame<MODE, EM>(T, P, d);
   s.px = f.px;
   s.py = f.py;
   s.pz = f.pz;
@@ -412,11 +440,11 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
 }
 
 // Emission (block 0) or step event of one photon.
-template <int MODE>
+template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ bool photon_event(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                              const PairCtx& c, Photon& s, bool& hit) {
   if (s.ctr3 < (1u << 8)) {
-    emit_event<MODE>(T, R, P, c, s);
+    emit_event<MODE, EM>(T, R, P, c, s);
     return true;
   }
   return step_event<MODE>(R, c, s, hit);
@@ -429,11 +457,11 @@ struct HitValues {
   float d0x, d0y, d0z;
 };
 
-template <int MODE>
+template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ HitValues hit_values(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                                 const PairCtx& c, const Photon& s) {
   const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, ctr_word(s.id, 0u));
-  const EmissionFrame f = emission_frame<MODE>(T, P, d);
+  const EmissionFrame f = emission_frame<MODE, EM>(T, P, d);
   HitValues h;
   h.wl = f.wl;
   emission_direction(f, d.u2, h.d0x, h.d0y, h.d0z);

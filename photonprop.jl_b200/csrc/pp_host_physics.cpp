@@ -3,6 +3,7 @@
 // tables that a context keeps resident on the device; they run once per
 // context, not per photon.
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "pp_internal.h"
@@ -177,6 +178,65 @@ double upper_incomplete_gamma(double s, double z) {
   return std::exp(lpre) * f;
 }
 
+// gamma(s, z), the lower incomplete gamma function: the power series below
+// z = s + 1, Gamma(s) - Gamma(s, z) above.
+double lower_incomplete_gamma(double s, double z) {
+  if (!(z > 0.0)) return 0.0;
+  if (z < s + 1.0) {
+    double term = 1.0 / s, sum = term;
+    for (int k = 1; k < 1000; ++k) {
+      term *= z / (s + k);
+      sum += term;
+      if (std::fabs(term) < std::fabs(sum) * 1e-17) break;
+    }
+    return std::exp(s * std::log(z) - z) * sum;
+  }
+  return std::tgamma(s) - upper_incomplete_gamma(s, z);
+}
+
+// Antiderivative of a exp(b |v|^c) + d: with k = -b,
+// sign(v) (a/c) k^(-1/c) gamma(1/c, k |v|^c) + d v.
+double cascade_G(double v) {
+  const double k = -kAngB, s = 1.0 / kAngC;
+  const double p = (kAngA / kAngC) * std::pow(k, -s) * lower_incomplete_gamma(s, k * std::pow(std::fabs(v), kAngC));
+  return (v < 0.0 ? -p : p) + kAngD * v;
+}
+
+void cascade_tables(double* fwd, double* inv) {
+  const double dv = (kCascVMax - kCascVMin) / kCascNF;
+  for (int i = 0; i <= kCascNF; ++i) fwd[i] = cascade_G(kCascVMin + dv * i);
+  const double g0 = fwd[0], g1 = fwd[kCascNF];
+  inv[0] = kCascVMin;
+  inv[kCascNI] = kCascVMax;
+  for (int j = 1; j < kCascNI; ++j) {
+    const double level = g0 + (g1 - g0) * j / kCascNI;
+    double lo = kCascVMin, hi = kCascVMax;
+    for (int it = 0; it < 64; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      if (cascade_G(mid) < level) lo = mid; else hi = mid;
+    }
+    inv[j] = 0.5 * (lo + hi);
+  }
+}
+
+// Inverse-CDF sample of cos(theta) at refractive index n: G at the ends of
+// [-1 - 1/n, 1 - 1/n] from the forward table, the level u of the way between
+// them, v from the inverse table (linear interpolation throughout).
+double cascade_sample(const double* fwd, const double* inv, double u, double n) {
+  const double c0 = 1.0 / n;
+  auto lerp_tab = [](const double* t, int cells, double x) {
+    x = std::min(std::max(x, 0.0), (double)cells);
+    int i = std::min((int)x, cells - 1);
+    return t[i] + (x - i) * (t[i + 1] - t[i]);
+  };
+  const double inv_dv = kCascNF / (kCascVMax - kCascVMin);
+  const double gl = lerp_tab(fwd, kCascNF, (-1.0 - c0 - kCascVMin) * inv_dv);
+  const double gh = lerp_tab(fwd, kCascNF, (1.0 - c0 - kCascVMin) * inv_dv);
+  const double g0 = fwd[0], g1 = fwd[kCascNF];
+  const double v = lerp_tab(inv, kCascNI, (gl + u * (gh - gl) - g0) * kCascNI / (g1 - g0));
+  return std::min(std::max(v + c0, -1.0), 1.0);
+}
+
 // The reference's antiderivative of a exp(b |x - cos_c|^c) + d
 // (src/emission.jl:65-81): with u = |x - cos_c| and k = -b,
 // F(x) = d x + (a / c) (cos_c - x) Gamma(1/c, k u^c) (k u^c)^(-1/c); above the
@@ -302,6 +362,18 @@ double pp_cherenkov_ang_dist_int(double ref_index) {
   double table[pp::kAngIntN];
   pp::cherenkov_ang_dist_int_table(table);
   return pp::ang_int_interp(table, ref_index);
+}
+
+double pp_cascade_cos_theta(double u, double n) {
+  static std::vector<double> fwd, inv;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    fwd.resize(pp::kCascNF + 1);
+    inv.resize(pp::kCascNI + 1);
+    pp::cascade_tables(fwd.data(), inv.data());
+  });
+  if (!(n > 0.0)) return NAN;
+  return pp::cascade_sample(fwd.data(), inv.data(), u, n);
 }
 
 pp_status pp_dir_reweight(const double* thetas, double obs_angle, const double* ref_ixs, double* out, int64_t n) {

@@ -37,6 +37,9 @@ size_t dev_tables_size();
 void fill_dev_tables(void* host_tables, const double coeffs[11], const float* knots, int n_knots,
                      const float* abs_wl, const float* abs_len, int n_abs, const float* pmt_wl,
                      const float* pmt_acc, int n_pmt);
+// Points the tables at the cascade emitter's device tables (kCascNF + 1
+// forward values, then kCascNI + 1 inverse values) with G's range.
+void set_cascade_tables(void* host_tables, const float* d_casc, double gmin, double gmax);
 void get_dev_knots(const void* host_tables, float* out, int* n);
 
 cudaError_t launch_chunk_scan(const LaunchArgs& a, cudaStream_t s);
@@ -76,6 +79,14 @@ double upper_incomplete_gamma(double s, double z);
 double cherenkov_ang_dist_int_closed(double ref_index, double lower, double upper);
 void cherenkov_ang_dist_int_table(double* out);
 double ang_int_interp(const double* table, double n);
+// Inverse-CDF tables of the cascade emitter: G(v) = integral of
+// a exp(b |v|^c) + d, v = cos(theta) - 1/n, on kCascNF + 1 uniform points of
+// [kCascVMin, kCascVMax], and v at kCascNI + 1 uniform levels of G.
+constexpr int kCascNF = 2048, kCascNI = 8192;
+constexpr double kCascVMin = -1.85, kCascVMax = 0.35;  // 1/n in [0.65, 0.85]
+double cascade_G(double v);
+void cascade_tables(double* fwd, double* inv);
+double cascade_sample(const double* fwd, const double* inv, double u, double ref_index);
 
 // fit stage (pp_fit.cu)
 struct FitConsts {

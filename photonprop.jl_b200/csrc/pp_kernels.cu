@@ -39,7 +39,7 @@ struct __align__(16) Staged {
   uint32_t pad;
 };
 
-template <int MODE, int WARPS>
+template <int MODE, int WARPS, int EM>
 __global__ void __launch_bounds__(WARPS * 32, 1024 / (WARPS * 32)) batched_kernel(const RunParams R) {
   __shared__ __align__(16) DevTables T;
   __shared__ Staged stage[WARPS][kStage];
@@ -100,6 +100,8 @@ __global__ void __launch_bounds__(WARPS * 32, 1024 / (WARPS * 32)) batched_kerne
                 if (R.chunk_offsets[mid] <= cid) lo = mid; else hi = mid - 1;
               }
               p = lo;
+              if (EM == kEmBasic && R.pairs[p].emitter == PP_EMITTER_CASCADE)
+                atomicOr(R.counters + 2, 4ull);  // a cascade pair in a launch without PP_OPT_CASCADE
               start = (cid - R.chunk_offsets[p]) * (unsigned long long)R.chunk;
               end = min(start + (unsigned long long)R.chunk, (unsigned long long)R.pairs[p].n_photons);
             }
@@ -135,7 +137,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1024 / (WARPS * 32)) batched_kerne
         const PairCtx pc = load_pair_ctx(P, ppair);
         Photon e;
         e.id = pid;
-        emit_event<MODE>(T, R, P, pc, e);
+        emit_event<MODE, EM>(T, R, P, pc, e);
         float4* dst = reinterpret_cast<float4*>(ring + ((r_head + r_count + lane) & (kStage - 1)));
         dst[0] = make_float4(e.px, e.py, e.pz, e.dx);
         dst[1] = make_float4(e.dy, e.dz, e.neg_ln2_len, e.max_dist);
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1024 / (WARPS * 32)) batched_kerne
     }
     if (__any_sync(kFull, hit)) {
       if (hit) {
-        const HitValues h = hit_values<MODE>(T, R, R.pairs + c.index, c, s);
+        const HitValues h = hit_values<MODE, EM>(T, R, R.pairs + c.index, c, s);
         record_hit_cached(R, ws, c, s, h);
       }
     }
@@ -194,7 +196,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1024 / (WARPS * 32)) batched_kerne
 
 // ---------------------------------------------------------------------------
 // Plain kernel: one pair, photons id = gtid + i * stride.
-template <int MODE>
+template <int MODE, int EM>
 __global__ void __launch_bounds__(512) plain_kernel(const RunParams R, const pp_pair* __restrict__ pair_ptr,
                                                     int pair_index) {
   __shared__ __align__(16) DevTables T;
@@ -215,9 +217,9 @@ __global__ void __launch_bounds__(512) plain_kernel(const RunParams R, const pp_
     while (alive) {
       bool hit = false;
       steps += (s.ctr3 >= (1u << 8));
-      alive = photon_event<MODE>(T, R, pair_ptr, c, s, hit);
+      alive = photon_event<MODE, EM>(T, R, pair_ptr, c, s, hit);
       if (hit) {
-        const HitValues h = hit_values<MODE>(T, R, pair_ptr, c, s);
+        const HitValues h = hit_values<MODE, EM>(T, R, pair_ptr, c, s);
         record_hit(R, c, s, h, 0);
       }
     }
@@ -261,9 +263,9 @@ __global__ void __launch_bounds__(1024) stacks_kernel(const RunParams R, const p
     while (alive) {
       bool hit = false;
       steps += (s.ctr3 >= (1u << 8));
-      alive = photon_event<MODE>(T, R, pair_ptr, c, s, hit);
+      alive = photon_event<MODE, kEmCascade>(T, R, pair_ptr, c, s, hit);
       if (hit) {
-        const HitValues h = hit_values<MODE>(T, R, pair_ptr, c, s);
+        const HitValues h = hit_values<MODE, kEmCascade>(T, R, pair_ptr, c, s);
         const int idx = atomicAdd(&cursor, 1);  // 1-based slot
         if (idx < ix_offset + stack_len) {
           const int j = idx - 1;
@@ -407,6 +409,7 @@ __global__ void eval_kernel(int op, const double* __restrict__ in, double* __res
     case 7: out[i] = (double)group_index(T, 1.f / (float)in[i]); break;
     case 8: out[i] = (double)scattering_length(T, (float)in[i]); break;
     case 9: out[i] = (double)interp_sorted((float)in[i], T.abs_wl, T.abs_len, T.n_abs); break;
+    case 11: out[i] = (double)cascade_cos_theta(T, 1.f / (float)in[2 * i + 1], (float)in[2 * i]); break;
     case 10:
       out[i] = T.n_pmt > 0 ? (double)interp_sorted((float)in[i], T.pmt_wl, T.pmt_acc, T.n_pmt) : 1.0;
       break;
@@ -524,6 +527,17 @@ void fill_dev_tables(void* host_tables, const double coeffs[11], const float* kn
   }
 }
 
+void set_cascade_tables(void* host_tables, const float* d_casc, double gmin, double gmax) {
+  ppd::DevTables* t = reinterpret_cast<ppd::DevTables*>(host_tables);
+  t->casc = d_casc;
+  t->casc_nf = kCascNF;
+  t->casc_ni = kCascNI;
+  t->casc_vmin = (float)kCascVMin;
+  t->casc_inv_dv = (float)(kCascNF / (kCascVMax - kCascVMin));
+  t->casc_gmin = (float)gmin;
+  t->casc_inv_dg = (float)(kCascNI / (gmax - gmin));
+}
+
 void get_dev_knots(const void* host_tables, float* out, int* n) {
   const ppd::DevTables* t = reinterpret_cast<const ppd::DevTables*>(host_tables);
   *n = t->n_knots;
@@ -544,16 +558,21 @@ cudaError_t launch_reset_counters(unsigned long long* counters, cudaStream_t s) 
 
 cudaError_t launch_batched(const LaunchArgs& a, int grid, int block, cudaStream_t s) {
   const ppd::RunParams R = to_params(a);
+  const bool casc = a.opts.mode == PP_MODE_PHYSICAL && (a.opts.flags & PP_OPT_CASCADE);
   if (block == 128) {
     if (a.opts.mode == PP_MODE_COMPAT)
-      ppd::batched_kernel<ppd::kCompat, 4><<<grid, 128, 0, s>>>(R);
+      ppd::batched_kernel<ppd::kCompat, 4, ppd::kEmBasic><<<grid, 128, 0, s>>>(R);
+    else if (casc)
+      ppd::batched_kernel<ppd::kPhysical, 4, ppd::kEmCascade><<<grid, 128, 0, s>>>(R);
     else
-      ppd::batched_kernel<ppd::kPhysical, 4><<<grid, 128, 0, s>>>(R);
+      ppd::batched_kernel<ppd::kPhysical, 4, ppd::kEmBasic><<<grid, 128, 0, s>>>(R);
   } else {
     if (a.opts.mode == PP_MODE_COMPAT)
-      ppd::batched_kernel<ppd::kCompat, 8><<<grid, 256, 0, s>>>(R);
+      ppd::batched_kernel<ppd::kCompat, 8, ppd::kEmBasic><<<grid, 256, 0, s>>>(R);
+    else if (casc)
+      ppd::batched_kernel<ppd::kPhysical, 8, ppd::kEmCascade><<<grid, 256, 0, s>>>(R);
     else
-      ppd::batched_kernel<ppd::kPhysical, 8><<<grid, 256, 0, s>>>(R);
+      ppd::batched_kernel<ppd::kPhysical, 8, ppd::kEmBasic><<<grid, 256, 0, s>>>(R);
   }
   count_launches(1);
   return cudaGetLastError();
@@ -563,9 +582,11 @@ cudaError_t launch_plain(const LaunchArgs& a, const pp_pair* d_pair, int pair_in
                          cudaStream_t s) {
   const ppd::RunParams R = to_params(a);
   if (a.opts.mode == PP_MODE_COMPAT)
-    ppd::plain_kernel<ppd::kCompat><<<grid, block, 0, s>>>(R, d_pair, pair_index);
+    ppd::plain_kernel<ppd::kCompat, ppd::kEmBasic><<<grid, block, 0, s>>>(R, d_pair, pair_index);
+  else if (a.opts.flags & PP_OPT_CASCADE)
+    ppd::plain_kernel<ppd::kPhysical, ppd::kEmCascade><<<grid, block, 0, s>>>(R, d_pair, pair_index);
   else
-    ppd::plain_kernel<ppd::kPhysical><<<grid, block, 0, s>>>(R, d_pair, pair_index);
+    ppd::plain_kernel<ppd::kPhysical, ppd::kEmBasic><<<grid, block, 0, s>>>(R, d_pair, pair_index);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -607,14 +628,14 @@ int batched_max_blocks_per_sm(int mode, int block) {
   int nb = 0;
   if (block == 128) {
     if (mode == PP_MODE_COMPAT)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kCompat, 4>, 128, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kCompat, 4, ppd::kEmBasic>, 128, 0);
     else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical, 4>, 128, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical, 4, ppd::kEmBasic>, 128, 0);
   } else {
     if (mode == PP_MODE_COMPAT)
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kCompat, 8>, 256, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kCompat, 8, ppd::kEmBasic>, 256, 0);
     else
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical, 8>, 256, 0);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical, 8, ppd::kEmBasic>, 256, 0);
   }
   return nb;
 }
@@ -622,9 +643,9 @@ int batched_max_blocks_per_sm(int mode, int block) {
 int plain_max_blocks_per_sm(int mode, int block) {
   int nb = 0;
   if (mode == PP_MODE_COMPAT)
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::plain_kernel<ppd::kCompat>, block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::plain_kernel<ppd::kCompat, ppd::kEmBasic>, block, 0);
   else
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::plain_kernel<ppd::kPhysical>, block, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::plain_kernel<ppd::kPhysical, ppd::kEmBasic>, block, 0);
   return nb;
 }
 

@@ -234,7 +234,7 @@ pp_status pp_particles_to_sources_device(pp_ctx* c, const pp_particle* d_parts, 
   std::lock_guard<std::mutex> lk(pp::ctx_mutex(c));
   if (mode != PP_LY_REFERENCE && mode != PP_LY_METRES)
     return pp::ctx_fail(c, PP_ERR_ARG, "unknown light-yield length mode");
-  if (emitter != PP_EMITTER_ISOTROPIC && emitter != PP_EMITTER_CHERENKOV_CONE)
+  if (emitter != PP_EMITTER_ISOTROPIC && emitter != PP_EMITTER_CHERENKOV_CONE && emitter != PP_EMITTER_CASCADE)
     return pp::ctx_fail(c, PP_ERR_ARG, "unknown emitter");
   if (!(wl_max > wl_min) || !(wl_min > 0.0)) return pp::ctx_fail(c, PP_ERR_ARG, "bad wavelength range");
   const int64_t ng = grid_points(len_min, len_max, precision);

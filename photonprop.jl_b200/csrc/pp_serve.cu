@@ -124,7 +124,8 @@ double expected_hits(const pp_pair& p) {
   const double dx = p.target[0] - cx, dy = p.target[1] - cy, dz = p.target[2] - cz;
   const double d = std::max(std::sqrt(dx * dx + dy * dy + dz * dz), (double)p.radius);
   const double r = p.radius;
-  const double f = p.emitter == PP_EMITTER_CHERENKOV_CONE ? 0.5 * r / d : r * r / (4.0 * d * d);
+  // cone and cascade emitters concentrate light near the Cherenkov angle: the cone bound for both
+  const double f = p.emitter != PP_EMITTER_ISOTROPIC ? 0.5 * r / d : r * r / (4.0 * d * d);
   return (double)p.n_photons * std::min(1.0, f);
 }
 
@@ -253,6 +254,11 @@ bool launch_slot(pp_server* S, Slot& s) {
   pp_run_opts o = S->cfg.opts;
   o.flags |= PP_OPT_COMPACT_HITS;
   o.flags &= ~(uint32_t)PP_OPT_NO_HITS;
+  for (int64_t i = 0; i < off; ++i)
+    if (hp[i].emitter == PP_EMITTER_CASCADE) {
+      o.flags |= PP_OPT_CASCADE;
+      break;
+    }
   const cudaStream_t st = s.stream;
   pp_status ps = PP_OK;
   if ((e = cudaMemcpyAsync(s.d_pairs.p, hp, (size_t)pairs * sizeof(pp_pair), cudaMemcpyHostToDevice, st)) ||
@@ -389,8 +395,9 @@ pp_status pp_server_submit(pp_server* S, const pp_pair* pairs, int32_t n_pairs, 
   for (int32_t i = 0; i < n_pairs; ++i) {
     const pp_pair& p = pairs[i];
     if (p.n_photons < 0 || p.n_photons > (1ll << 40) || !(p.radius > 0.f) ||
-        (p.emitter != PP_EMITTER_ISOTROPIC && p.emitter != PP_EMITTER_CHERENKOV_CONE) ||
-        (p.emitter == PP_EMITTER_CHERENKOV_CONE && S->cfg.opts.mode == PP_MODE_COMPAT))
+        (p.emitter != PP_EMITTER_ISOTROPIC && p.emitter != PP_EMITTER_CHERENKOV_CONE &&
+         p.emitter != PP_EMITTER_CASCADE) ||
+        (p.emitter != PP_EMITTER_ISOTROPIC && S->cfg.opts.mode == PP_MODE_COMPAT))
       return PP_ERR_ARG;
     hits += std::ceil(S->cfg.hit_safety * expected_hits(p)) + 64.0;
     r->photons += (double)p.n_photons;

@@ -18,9 +18,9 @@ PP_OK, PP_ERR_ARG, PP_ERR_OOM, PP_ERR_OVERFLOW, PP_ERR_TIMEOUT, PP_ERR_CUDA, PP_
 STATUS_NAMES = {0: "PP_OK", 1: "PP_ERR_ARG", 2: "PP_ERR_OOM", 3: "PP_ERR_OVERFLOW", 4: "PP_ERR_TIMEOUT",
                 5: "PP_ERR_CUDA", 6: "PP_ERR_STATE", 7: "PP_ERR_BUSY"}
 MODE_COMPAT, MODE_PHYSICAL = 0, 1
-EMITTER_ISOTROPIC, EMITTER_CHERENKOV_CONE = 0, 1
+EMITTER_ISOTROPIC, EMITTER_CHERENKOV_CONE, EMITTER_CASCADE = 0, 1, 2
 SPECTRUM_CHERENKOV, SPECTRUM_MONOCHROMATIC = 0, 1
-OPT_PMT_WEIGHT, OPT_NORMALIZE, OPT_NO_HITS, OPT_COMPACT_HITS = 1, 2, 4, 8
+OPT_PMT_WEIGHT, OPT_NORMALIZE, OPT_NO_HITS, OPT_COMPACT_HITS, OPT_CASCADE = 1, 2, 4, 8, 16
 MAX_KNOTS, MAX_ABS, MAX_PMT, N_STATS = 64, 32, 256, 8
 NOALLOC_MAX_PAIRS = 65536
 
@@ -128,6 +128,7 @@ _SIGS = [
     ("pp_cherenkov_ang_dist_int_exact", _D, [_D, _D, _D]),
     ("pp_cherenkov_ang_dist_int", _D, [_D]),
     ("pp_dir_reweight", ctypes.c_int, [_VP, _D, _VP, _VP, _I64]),
+    ("pp_cascade_cos_theta", _D, [_D, _D]),
     ("pp_propagate_fit", ctypes.c_int, [_VP, _VP, _I64, ctypes.POINTER(RunOpts), _VP, _I32, _I64,
                                         ctypes.POINTER(_I64), _VP, _VP, _VP, _VP]),
     ("pp_fit_hits_device", ctypes.c_int, [_VP, _VP, _I64, _I32, _VP, _I64, _VP, _VP, _I32, _VP, _VP, _VP]),

@@ -12,7 +12,9 @@ from .spectrum import Spectrum
 @dataclass(frozen=True)
 class AngularEmissionProfile:
     """AngularEmissionProfile{U,T}, src/emission.jl:13: a tag for the angular
-    emission model ("IsotropicEmission" or "CherenkovEmission")."""
+    emission model: "IsotropicEmission", "CherenkovEmission" (a track emitting
+    on the Cherenkov cone) or "CherenkovAngularEmission" (a point emitting
+    with the EM-cascade profile cherenkov_ang_dist about its direction)."""
 
     kind: str = "IsotropicEmission"
 
@@ -22,11 +24,14 @@ class AngularEmissionProfile:
             return _lib.EMITTER_ISOTROPIC
         if self.kind == "CherenkovEmission":
             return _lib.EMITTER_CHERENKOV_CONE
+        if self.kind == "CherenkovAngularEmission":
+            return _lib.EMITTER_CASCADE
         raise ValueError(f"Cannot initialize {self.kind}")
 
 
 IsotropicEmission = AngularEmissionProfile("IsotropicEmission")
 CherenkovEmission = AngularEmissionProfile("CherenkovEmission")
+CherenkovAngularEmission = AngularEmissionProfile("CherenkovAngularEmission")
 
 
 @dataclass

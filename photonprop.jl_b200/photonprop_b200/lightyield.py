@@ -149,7 +149,8 @@ def particles_to_sources(propagator, particles, len_range, precision, wl_range=(
     import torch
     parts = particles if isinstance(particles, np.ndarray) else particles_array(particles)
     parts = np.ascontiguousarray(parts, dtype=_lib.PARTICLE_DTYPE)
-    em = {"isotropic": _lib.EMITTER_ISOTROPIC, "cone": _lib.EMITTER_CHERENKOV_CONE}[emitter]
+    em = {"isotropic": _lib.EMITTER_ISOTROPIC, "cone": _lib.EMITTER_CHERENKOV_CONE,
+          "cascade": _lib.EMITTER_CASCADE}[emitter]
     dev = torch.device("cuda", propagator.device)
     n_grid_est = int(np.floor((len_range[1] - len_range[0]) / precision * (1 + 1e-12) + 1e-9)) + 1
     cap = max(1, len(parts) * max(n_grid_est - 1, 0))

@@ -42,6 +42,7 @@ class RunOptions:
     pmt_weight: bool | None = None
     normalize: bool = False
     write_hits: bool = True
+    cascade: bool = False  # the device entry points' pairs may include cascade emitters
     block_size: int = 0
     blocks_per_sm: int = 0
     chunk_photons: int = 0
@@ -69,6 +70,8 @@ class RunOptions:
             flags |= _lib.OPT_NORMALIZE
         if not self.write_hits:
             flags |= _lib.OPT_NO_HITS
+        if self.cascade:
+            flags |= _lib.OPT_CASCADE
         o.flags = flags
         o.block_size, o.blocks_per_sm, o.chunk_photons = self.block_size, self.blocks_per_sm, self.chunk_photons
         return o

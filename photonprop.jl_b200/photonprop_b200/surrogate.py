@@ -102,7 +102,9 @@ def gemm_selftest(a_bf16_u16, b_bf16_u16, device=0):
 
 
 def features(pairs) -> np.ndarray:
-    """[n, 4] raw features of pairs: log10 d, cos angle, log10 N, emitter flag."""
+    """[n, 4] raw features of pairs: log10 d, cos angle, log10 N, emitter flag
+    (0 isotropic, 1 Cherenkov cone, 2 cascade profile: outside the trained
+    range, so the MC kernel answers)."""
     p = np.asarray(pairs)
     pos = p["pos"].astype(np.float64)
     d = p["dir"].astype(np.float64)
@@ -111,7 +113,8 @@ def features(pairs) -> np.ndarray:
     v = p["target"].astype(np.float64) - src
     dist = np.linalg.norm(v, axis=1)
     cosang = np.einsum("ij,ij->i", v / dist[:, None], d)
-    return np.stack([np.log10(dist), cosang, np.log10(np.maximum(p["n_photons"], 1)), cone.astype(np.float64)],
+    flag = np.where(p["emitter"] == _lib.EMITTER_CASCADE, 2.0, cone.astype(np.float64))
+    return np.stack([np.log10(dist), cosang, np.log10(np.maximum(p["n_photons"], 1)), flag],
                     axis=1).astype(np.float32)
 
 

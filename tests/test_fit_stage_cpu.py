@@ -95,3 +95,24 @@ def test_fit_table_parquet_round_trip(tmp_path):
     t = tr[("det_fraction", "log_det_fraction_scaled")]
     x = d32["det_fraction"].to_numpy().astype(np.float64)
     np.testing.assert_allclose(md.reverse_transformation(md.apply_transformation(x, t), t), x, rtol=1e-12)
+
+
+def test_cascade_sampler_matches_oracle_and_profile():
+    """The library's FP64 cascade sampler equals the oracle's (independent
+    tables), and samples drawn on a fine grid of u follow the normalised
+    profile a exp(b |x - 1/n|^c) + d on [-1, 1] (quadrature CDF)."""
+    L = pp._lib.load()
+    rng = np.random.default_rng(3)
+    for u, n in zip(rng.uniform(size=200), rng.uniform(1.3, 1.4, size=200)):
+        assert L.pp_cascade_cos_theta(u, n) == pytest.approx(float(F.cascade_cos_theta(u, n)), abs=1e-12)
+    n = 1.34
+    us = (np.arange(200000) + 0.5) / 200000
+    x = np.sort(F.cascade_cos_theta(us, np.full_like(us, n)))
+    f = lambda t: F.cherenkov_ang_dist(t, n)
+    c0 = 1 / n
+    tot = integrate.quad(f, -1, c0, limit=200)[0] + integrate.quad(f, c0, 1, limit=200)[0]
+    for q in (-0.5, 0.0, 0.5, 0.7, c0, 0.78, 0.9):
+        cdf = (integrate.quad(f, -1, min(q, c0), limit=200)[0]
+               + (integrate.quad(f, c0, q, limit=200)[0] if q > c0 else 0.0)) / tot
+        assert np.searchsorted(x, q) / len(x) == pytest.approx(cdf, abs=2e-4)
+

@@ -410,3 +410,52 @@ def test_full_size_benchmark_batch_properties(propagator):
     inwin = (t >= 0) & (t < 1000.0)
     np.testing.assert_allclose(a.hist.sum(axis=1), np.bincount(ha["pair"][inwin], weights=w[inwin],
                                                                minlength=len(b)), rtol=1e-5, atol=1e-9)
+
+
+def test_cascade_emitter_sampler_matches_oracle(propagator):
+    """cos(theta) of the cascade emitter: the device's FP32 tables against the
+    oracle's FP64 tables (built independently with scipy)."""
+    from oracle import fits as F
+    rng = np.random.default_rng(21)
+    u = rng.uniform(size=20000)
+    n = rng.uniform(1.30, 1.40, size=20000)
+    got = propagator.device_eval(11, np.stack([u, n], axis=1))[:, 0]
+    np.testing.assert_allclose(got, F.cascade_cos_theta(u, n), rtol=0, atol=3e-5)
+
+
+def test_fixed_rng_cascade_emitter(propagator, oracle_tables):
+    b = pp.batches.mixed_batch(32, seed=17, n_min=2e4, n_max=2e5, d_min=2.0, d_max=8.0)
+    b["emitter"] = pp._lib.EMITTER_CASCADE
+    b["track_len"] = 0.0
+    ro = pp.RunOptions(mode="physical", g=0.95, t_max=300.0, hist_bins=300)
+    res = propagator.propagate(b, ro)
+    h, s, hist, steps, total = O.propagate(oracle_tables, to_oracle_pairs(b), to_oracle_opts(ro))
+    assert total > 200
+    g, o, ng, no = match_hits(res.hits, h)
+    _check_matched(g, o, ng, no, "physical-cascade")
+    # compat mode has no cascade emitter (the reference rejects non-isotropic emission)
+    with pytest.raises(pp.PPError):
+        propagator.propagate(b[:1], pp.RunOptions(mode="compat"))
+
+
+def test_cascade_pairs_on_the_device_api_need_the_flag(propagator):
+    import torch
+    b = pp.batches.mixed_batch(8, seed=19, n_min=1e5, n_max=2e5, d_min=2.0, d_max=4.0)
+    b["emitter"] = pp._lib.EMITTER_CASCADE
+    ref = propagator.propagate(b, pp.RunOptions(mode="physical", hist_bins=0))
+    d_pairs = torch.from_numpy(b.view(np.uint8).copy()).cuda()
+    cap = 1 << 18
+    d_hits = torch.zeros(cap * 64, dtype=torch.uint8, device="cuda")
+    d_cnt = torch.zeros(4, dtype=torch.int64, device="cuda")
+    d_st = torch.zeros((len(b), 8), dtype=torch.float64, device="cuda")
+    for flag in (False, True):
+        ro = pp.RunOptions(mode="physical", hist_bins=0, cascade=flag)
+        propagator.propagate_device(d_pairs, len(b), ro, d_hits, cap, d_cnt, d_st, None,
+                                    stream=torch.cuda.current_stream())
+        torch.cuda.synchronize()
+        status = int(d_cnt[2].item())
+        if flag:
+            assert status & 4 == 0
+            np.testing.assert_allclose(d_st.cpu().numpy(), ref.stats, rtol=1e-9, atol=1e-12)
+        else:
+            assert status & 4  # flagged: emitted on the cone instead
