@@ -23,9 +23,12 @@ const PP_MODE_COMPAT = Cint(0)
 const PP_MODE_PHYSICAL = Cint(1)
 const PP_EMITTER_ISOTROPIC = Cint(0)
 const PP_EMITTER_CHERENKOV_CONE = Cint(1)
+const PP_EMITTER_CASCADE = Cint(2)          # CherenkovAngularEmission, physical mode
 const PP_OPT_PMT_WEIGHT = UInt32(1)
 const PP_OPT_NORMALIZE = UInt32(2)
 const PP_OPT_NO_HITS = UInt32(4)
+const PP_OPT_COMPACT_HITS = UInt32(8)
+const PP_OPT_CASCADE = UInt32(16)
 const PP_STATS = 8
 
 struct PPMediumDesc            # WaterProperties (src/medium.jl:23-50) + absorption table
