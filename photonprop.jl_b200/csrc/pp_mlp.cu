@@ -802,8 +802,11 @@ pp_status pp_mlp_create(int device, uint64_t seed, pp_mlp** out) {
       (e = cudaMalloc(&m->d_tc, 4 * mlp::TILE_BYTES)) || (e = cudaMalloc(&m->d_norm, 32 * 4)) ||
       (e = cudaMalloc(&m->d_error, 16)) || (e = cudaMalloc(&m->d_loss, 16))) {
     cudaGetLastError();
+    for (void* b : {(void*)m->d_params, (void*)m->d_grad, (void*)m->d_m, (void*)m->d_v, (void*)m->d_w1r,
+                    (void*)m->d_w4r, (void*)m->d_tc, (void*)m->d_norm, (void*)m->d_error, (void*)m->d_loss})
+      if (b) cudaFree(b);
     delete m;
-    return PP_ERR_OOM;
+    return e == cudaErrorMemoryAllocation ? PP_ERR_OOM : PP_ERR_CUDA;
   }
   // Glorot-uniform weights, zero biases, from a splitmix64 stream of `seed`
   std::vector<float> p(mlp::N_PARAMS, 0.f);

@@ -240,7 +240,7 @@ bool launch_slot(pp_server* S, Slot& s) {
       (e = s.h_counters.ensure(64)) || (e = s.h_stats.ensure((size_t)pairs * PP_STATS * sizeof(double))) ||
       (e = s.h_hist.ensure((size_t)pairs * std::max(bins, 1) * sizeof(double)))) {
     cudaGetLastError();
-    fail_requests(S, take, PP_ERR_OOM);
+    fail_requests(S, take, e == cudaErrorMemoryAllocation ? PP_ERR_OOM : PP_ERR_CUDA);
     return true;
   }
   s.pair_start.clear();
