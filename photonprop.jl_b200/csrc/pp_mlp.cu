@@ -977,7 +977,9 @@ pp_status pp_mlp_gemm_selftest(int device, const uint16_t* a_bf16, const uint16_
   if ((e = cudaMalloc(&da, 128 * 128 * 2)) || (e = cudaMalloc(&db, 128 * 128 * 2)) ||
       (e = cudaMalloc(&dc, 128 * 128 * 4)) || (e = cudaMalloc(&de, 16))) {
     cudaGetLastError();
-    return PP_ERR_OOM;
+    for (void* b : {da, db, dc, de})
+      if (b) cudaFree(b);
+    return e == cudaErrorMemoryAllocation ? PP_ERR_OOM : PP_ERR_CUDA;
   }
   cudaFuncSetAttribute(mlp::gemm_test_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)mlp::kTestSmem);
   int flag = 0;
