@@ -554,8 +554,8 @@ def fits_cpu_baseline(pairs, angles, knots, target_seconds):
 
 def run_event(args):
     """--workload event: one 100 GeV electron cascade at the origin along +z
-    -> Cherenkov track sources every 0.1 m over 20 m (light-yield kernel,
-    metres mode) -> every source with every module of a 5 x 5 string
+    -> point sources with the cascade angular profile every 0.1 m over 20 m
+    (light-yield kernel, metres mode) -> every source with every module of a 5 x 5 string
     detector (20 m string spacing, 20 modules 5 m apart, r = 0.21 m) ->
     batched propagation (physical mode).  Everything stays on the device;
     each stage is timed with CUDA events."""
@@ -571,7 +571,7 @@ def run_event(args):
     xs = np.arange(-40.0, 40.1, 20.0)
     mods = np.array([[x, y, z, 0.21] for x in xs for y in xs for z in np.arange(-40.0, 55.1, 5.0)],
                     dtype=np.float32)
-    ro = pp.RunOptions(mode="physical", g=0.95, t_max=1000.0, hist_bins=1000)
+    ro = pp.RunOptions(mode="physical", g=0.95, t_max=1000.0, hist_bins=1000, cascade=True)
     L = pp._lib.load()
     with pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=0) as prop:
         n_src_cap = 400
@@ -583,7 +583,7 @@ def run_event(args):
         # sizes first (one untimed pass)
         pp._lib.check(L.pp_particles_to_sources_device(prop.handle, d_parts.data_ptr(), 1, 0.0, 20.0, 0.1,
                                                        pp._lib.LY_METRES, 300.0, 800.0,
-                                                       pp._lib.EMITTER_CHERENKOV_CONE, d_src.data_ptr(), n_src_cap,
+                                                       pp._lib.EMITTER_CASCADE, d_src.data_ptr(), n_src_cap,
                                                        ctypes.byref(ng), s.cuda_stream), prop.handle)
         n_src = int(ng.value) - 1
         n_pairs = n_src * len(mods)
@@ -599,7 +599,7 @@ def run_event(args):
             ev[0].record(s)
             pp._lib.check(L.pp_particles_to_sources_device(prop.handle, d_parts.data_ptr(), 1, 0.0, 20.0, 0.1,
                                                            pp._lib.LY_METRES, 300.0, 800.0,
-                                                           pp._lib.EMITTER_CHERENKOV_CONE, d_src.data_ptr(),
+                                                           pp._lib.EMITTER_CASCADE, d_src.data_ptr(),
                                                            n_src_cap, ctypes.byref(ng), s.cuda_stream), prop.handle)
             ev[1].record(s)
             pp._lib.check(L.pp_cross_pairs_device(prop.handle, d_src.data_ptr(), n_src, d_mods.data_ptr(), len(mods),
@@ -615,7 +615,7 @@ def run_event(args):
     t = np.median(np.array(times[1:]), axis=0)
     line = {"metric": "event-driven batch: cascade -> sources -> pairs -> propagation, photons/s", "unit": UNIT,
             "value": photons / (t.sum() / 1e3), "n_gpus": 1, "data": "synthetic", "higher_is_better": True,
-            "config": {"workload": "100 GeV e- cascade along +z, Cherenkov track sources every 0.1 m over 20 m, "
+            "config": {"workload": "100 GeV e- cascade along +z, cascade-profile point sources every 0.1 m over 20 m, "
                                    f"{len(mods)} modules (5 x 5 strings, 20 m spacing, 20 modules 5 m apart), "
                                    "physical mode, 1000 x 1 ns histograms"},
             "sources": n_src, "pairs": n_pairs, "photons": photons, "hits": hits,
@@ -625,8 +625,8 @@ def run_event(args):
 
 
 def run_llh(args):
-    """--workload llh: the event of --workload event (100 GeV e-, 200 cone
-    sources x 500 modules) observed once by the MC kernel (each weighted hit
+    """--workload llh: the event of --workload event (100 GeV e-, 200
+    cascade-profile sources x 500 modules) observed once by the MC kernel (each weighted hit
     kept with probability = its weight), per-(source, module) hypothesis
     parameters from an independent MC run (expected photons + Gamma-mixture
     fit of each pair), then the extended likelihood of 64 energy hypotheses
@@ -648,7 +648,7 @@ def run_llh(args):
     part = ly.Particle((0.0, 0.0, 0.0), (0.0, 0.0, 1.0), 0.0, 100.0, ly.ParticleType.EMinus)
     ro = pp.RunOptions(mode="physical", g=0.95, t_max=1000.0, hist_bins=1000)
     with pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=0) as prop:
-        src, _ = ly.particles_to_sources(prop, [part], (0.0, 20.0), 0.1, mode="metres", emitter="cone")
+        src, _ = ly.particles_to_sources(prop, [part], (0.0, 20.0), 0.1, mode="metres", emitter="cascade")
         S, M = len(src), len(mods)
         obs_pairs = ly.cross_pairs(prop, src, mods, seed=11)
         t0 = time.perf_counter()
@@ -693,7 +693,7 @@ def run_llh(args):
     line = {"metric": "event likelihood hypotheses/s (surrogate parameters + FP64 likelihood kernel)",
             "value": 1.0 / per_hyp, "unit": "hypotheses/s", "n_gpus": 1, "higher_is_better": True,
             "data": "synthetic",
-            "config": {"workload": f"100 GeV e- cascade, {S} cone sources x {M} modules, {int(counts.sum())} "
+            "config": {"workload": f"100 GeV e- cascade, {S} cascade-profile sources x {M} modules, {int(counts.sum())} "
                                    f"observed hits, {H} energy hypotheses per launch (x0.5 .. x2)"},
             "llh_kernel_s_per_launch": t_llh, "llh_hypotheses_per_s": H / t_llh,
             "surrogate_queries_per_hypothesis": S * M, "surrogate_queries_per_s": inf["queries_per_s"],

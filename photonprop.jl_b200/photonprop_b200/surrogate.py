@@ -154,6 +154,7 @@ def mc_dataset(prop: Propagator, pairs, opts: RunOptions, min_hits_mu=1, min_hit
     cols = {k: [] for k in ("x", "y", "m", "h", "mu", "sg", "hist", "ts")}
     o = RunOptions(**{**opts.__dict__})
     o.write_hits = False
+    o.cascade = o.cascade or bool(np.any(np.asarray(pairs["emitter"]) == _lib.EMITTER_CASCADE))
     for s0 in range(0, len(pairs), chunk):
         b = np.ascontiguousarray(pairs[s0:s0 + chunk])
         n = len(b)
