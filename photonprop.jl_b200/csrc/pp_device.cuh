@@ -270,7 +270,7 @@ struct Photon {
 };
 
 struct PairCtx {
-  float tx, ty, tz, r2;
+  float tx, ty, tz, r;  // sphere centre and radius
   uint32_t seed_lo, seed_hi;
   int32_t index;
 };
@@ -282,7 +282,7 @@ __device__ __forceinline__ PairCtx load_pair_ctx(const pp_pair* __restrict__ P, 
   c.tx = t.x;
   c.ty = t.y;
   c.tz = t.z;
-  c.r2 = t.w * t.w;
+  c.r = t.w;
   c.seed_lo = sd.x;
   c.seed_hi = sd.y;
   c.index = index;
@@ -409,7 +409,7 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
   const float ex = s.px - c.tx, ey = s.py - c.ty, ez = s.pz - c.tz;
   const float a = fmaf(s.dz, ez, fmaf(s.dy, ey, s.dx * ex));
   const float pp = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-  const float b = fmaf(a, a, c.r2 - pp);
+  const float b = fmaf(a, a, fmaf(c.r, c.r, -pp));
   // branch-free decisions: the line meets the sphere (b >= 0) at dd ahead
   const float dd = -a - sqrt_a(fmaxf(b, 0.f));
   const bool line = b >= 0.f;
@@ -421,7 +421,12 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
     alive = !geo;
   } else {
     hit = geo && s.dist + dd <= s.max_dist;  // arrives inside the time window
-    move = !geo && s.dist + step <= s.max_dist;
+    // A photon farther from the sphere than the path it has left before t_max
+    // can never arrive in time (any path to the sphere is at least the straight
+    // distance): it ends now.  Exact, with a margin for FP32 rounding; it
+    // spares the steps of photons drifting away from their target.
+    const float reach = fmaf(s.max_dist - s.dist, 1.0001f, c.r + 0.05f);
+    move = !geo && s.dist + step <= s.max_dist && pp <= reach * reach;
     alive = move;
   }
   const float len = hit ? dd : (move ? step : 0.f);

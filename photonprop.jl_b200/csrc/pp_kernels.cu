@@ -73,7 +73,7 @@ __global__ void __launch_bounds__(WARPS * 32, 1024 / (WARPS * 32)) batched_kerne
   s.px = s.py = s.pz = s.dx = s.dy = s.dist = s.neg_ln2_len = s.max_dist = 0.f;
   s.dz = 1.f;
   PairCtx c;
-  c.tx = c.ty = c.tz = c.r2 = 0.f;
+  c.tx = c.ty = c.tz = c.r = 0.f;
   c.seed_lo = c.seed_hi = 0u;
   c.index = 0;
   unsigned steps = 0;
