@@ -459,3 +459,18 @@ def test_cascade_pairs_on_the_device_api_need_the_flag(propagator):
             np.testing.assert_allclose(d_st.cpu().numpy(), ref.stats, rtol=1e-9, atol=1e-12)
         else:
             assert status & 4  # flagged: emitted on the cone instead
+
+
+def test_reachability_cut_is_exact(propagator, oracle_tables):
+    """Physical mode ends a photon once its sphere is farther than the path it
+    has left before t_max.  With t_max = 100 ns (about 22 m of path) and
+    spheres 10-20 m away most photons end that way; the oracle, which steps
+    every photon to t_max, must find exactly the same hits."""
+    b = pp.batches.mixed_batch(24, seed=23, n_min=2e5, n_max=5e5, d_min=10.0, d_max=20.0)
+    ro = pp.RunOptions(mode="physical", g=0.95, t_max=100.0, hist_bins=100)
+    res = propagator.propagate(b, ro)
+    h, s, hist, steps, total = O.propagate(oracle_tables, to_oracle_pairs(b), to_oracle_opts(ro))
+    assert total > 100
+    g, o, ng, no = match_hits(res.hits, h)
+    assert ng == 0 and no == 0, (ng, no)
+    _check_matched(g, o, ng, no, "physical-cut")
