@@ -408,8 +408,13 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
   const float step = lg2(d.u0) * s.neg_ln2_len;
   const float ex = s.px - c.tx, ey = s.py - c.ty, ez = s.pz - c.tz;
   const float a = fmaf(s.dz, ez, fmaf(s.dy, ey, s.dx * ex));
-  const float pp = fmaf(ez, ez, fmaf(ey, ey, ex * ex));
-  const float b = fmaf(a, a, fmaf(c.r, c.r, -pp));
+  // b = a^2 - |e|^2 + r^2 (src/photon_prop_cuda.jl:340) evaluated as r^2 - |e - a d|^2:
+  // the same number, but without cancelling two large squares, which in FP32
+  // costs millimetres at grazing incidence on a sphere tens of metres away
+  const float qx = fmaf(-a, s.dx, ex), qy = fmaf(-a, s.dy, ey), qz = fmaf(-a, s.dz, ez);
+  const float q = fmaf(qz, qz, fmaf(qy, qy, qx * qx));
+  const float b = fmaf(c.r, c.r, -q);
+  const float pp = fmaf(a, a, q);  // |e|^2
   // branch-free decisions: the line meets the sphere (b >= 0) at dd ahead
   const float dd = -a - sqrt_a(fmaxf(b, 0.f));
   const bool line = b >= 0.f;
