@@ -686,7 +686,9 @@ def run_llh(args):
             e1.record(st)
             torch.cuda.synchronize()
             tl.append(e0.elapsed_time(e1) / 1e3)
-        llh = d_l.cpu().numpy().sum(axis=1)
+        per_mod = d_l.cpu().numpy()
+        finite = np.all(np.isfinite(per_mod), axis=0)  # a hit no source can produce gives ln f = -inf
+        llh = per_mod[:, finite].sum(axis=1)
         inf = surrogate_inference_rate(0, S * M)
     t_llh = float(np.median(tl[1:]))
     per_hyp = t_llh / H + S * M / inf["queries_per_s"]
@@ -698,7 +700,8 @@ def run_llh(args):
             "llh_kernel_s_per_launch": t_llh, "llh_hypotheses_per_s": H / t_llh,
             "surrogate_queries_per_hypothesis": S * M, "surrogate_queries_per_s": inf["queries_per_s"],
             "mc_seconds_per_hypothesis": t_mc, "speedup_vs_mc": t_mc / per_hyp,
-            "best_scale": float(scales[int(np.argmax(llh))])}
+            "best_scale": float(scales[int(np.argmax(llh))]),
+            "modules_with_an_impossible_hit": int((~finite).sum())}
     print(json.dumps(line), flush=True)
 
 

@@ -121,6 +121,7 @@ struct pp_ctx {
   // fit stage: constants and device buffers
   pp::FitConsts fitk;
   DevBuf fit_counts, fit_rec, fit_moments, fit_out, fit_cs;
+  DevBuf llh_chunks;  // event likelihood: first hit chunk of every module
 
   pp_status fail(pp_status s, const std::string& msg) {
     err = msg;
@@ -465,7 +466,7 @@ void pp_destroy(pp_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->drop_graphs();
     for (DevBuf* b : {&c->pairs, &c->hits, &c->counters, &c->stats, &c->hist, &c->offsets, &c->queue, &c->fit_counts,
-                      &c->fit_rec, &c->fit_moments, &c->fit_out, &c->fit_cs})
+                      &c->fit_rec, &c->fit_moments, &c->fit_out, &c->fit_cs, &c->llh_chunks})
       b->release();
     if (c->d_tables) cudaFree(c->d_tables);
     if (c->d_casc) cudaFree(c->d_casc);
@@ -1121,6 +1122,12 @@ const pp_medium_desc* ctx_medium(const pp_ctx* c) { return &c->medium; }
 pp_status ctx_fail(pp_ctx* c, pp_status s, const char* msg) { return c->fail(s, msg); }
 pp_status ctx_cuda_fail(pp_ctx* c, cudaError_t e, const char* where) { return c->cuda_fail(e, where); }
 std::mutex& ctx_mutex(pp_ctx* c) { return c->mu; }
+cudaError_t ctx_llh_scratch(pp_ctx* c, size_t bytes, void** out) {
+  bool grew = false;
+  cudaError_t e = ensure(c->llh_chunks, bytes, &grew);
+  *out = c->llh_chunks.p;
+  return e;
+}
 }  // namespace pp
 
 // ---------------------------------------------------------------------------

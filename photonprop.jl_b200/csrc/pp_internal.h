@@ -68,6 +68,7 @@ const pp_medium_desc* ctx_medium(const pp_ctx* c);
 pp_status ctx_fail(pp_ctx* c, pp_status s, const char* msg);
 pp_status ctx_cuda_fail(pp_ctx* c, cudaError_t e, const char* where);
 std::mutex& ctx_mutex(pp_ctx* c);
+cudaError_t ctx_llh_scratch(pp_ctx* c, size_t bytes, void** out);  // caller holds the context mutex
 
 // Cherenkov angular distribution of EM cascades, e- parameters
 // (src/emission.jl:19), and the reference's table of its [-1, 1] integral
