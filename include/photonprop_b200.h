@@ -288,10 +288,12 @@ PP_API pp_status pp_cuda_propagate_photons(pp_ctx* ctx, float* d_out_positions,
  * (theta0 the emission polar angle, n the phase index at the photon's
  * wavelength), multiplied by the hit weight, and a Gamma distribution is
  * fitted by maximum likelihood to the weighted arrival-time residuals
- * tres = t - (|target - source| - r) n(800 nm) / c with tres >= 0.  The
+ * tres = t - (|target - source| - r) n(800 nm) / c.  The
  * detection fraction is the summed weight of all hits over the photons
- * generated. */
-#define PP_FIT_MOMENTS 4 /* per (pair, angle): sum w (all hits), then over tres >= 0:
+ * generated.  The fit takes tres > 0 (the reference's mask is tres >= 0: a
+ * residual of exactly 0, which FP32 rounding makes common for photons that
+ * fly straight at the sphere, has no Gamma likelihood). */
+#define PP_FIT_MOMENTS 4 /* per (pair, angle): sum w (all hits), then over tres > 0:
                             sum w, sum w tres, sum w ln(tres) */
 #define PP_FIT_OUT 3     /* per (pair, angle): fit_alpha, fit_theta, det_fraction */
 #define PP_MAX_FIT_ANGLES 4096
@@ -318,7 +320,7 @@ PP_API pp_status pp_dir_reweight(const double* thetas, double obs_angle, const d
  * device for every pair and each of the n_angles observation angles
  * (radians, host array): fits = n_pairs x n_angles x PP_FIT_OUT doubles
  * (fit_alpha and fit_theta of the weighted Gamma maximum-likelihood fit, NaN
- * where no hit has tres >= 0; det_fraction); moments (may be NULL) =
+ * where no hit has tres > 0; det_fraction); moments (may be NULL) =
  * n_pairs x n_angles x PP_FIT_MOMENTS; stats / hist as pp_propagate (may be
  * NULL); *n_hits = all hits.  hit_capacity sizes the device hit buffer:
  * pairs run in waves whose hits fit it (a wave that overflows is repacked

@@ -115,10 +115,11 @@ def gamma_fit(x, w):
 
 
 def moments(tres, weight):
-    """[sum w (all), sum w, sum w tres, sum w ln tres] (tres >= 0)."""
+    """[sum w (all), sum w, sum w tres, sum w ln tres] over tres > 0 (the
+    reference masks tres >= 0; an exact 0 has no Gamma likelihood)."""
     tres = np.asarray(tres, dtype=np.float64)
     w = np.asarray(weight, dtype=np.float64)
-    m = tres >= 0
+    m = tres > 0
     with np.errstate(divide="ignore", invalid="ignore"):
         lt = np.where(m, np.log(np.where(m, tres, 1.0)), 0.0)
     return np.array([w.sum(), w[m].sum(), (w[m] * tres[m]).sum(), (w[m] * lt[m]).sum()])

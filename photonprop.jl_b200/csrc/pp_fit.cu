@@ -99,9 +99,12 @@ __device__ __forceinline__ float ang_norm(const pp::FitConsts& K, float n) {
   return 2.f * fmaf(K.normf[i + 1] - K.normf[i], f, K.normf[i]);
 }
 
+// The fit takes tres > 0 (the reference masks tres >= 0, src/modelling.jl:73,
+// but a residual of exactly 0, which FP32 rounding makes common for photons
+// that fly straight at the sphere, has ln 0 = -inf and no Gamma likelihood).
 __device__ __forceinline__ void write_rec(pp::FitRec* r, float ct, float st, float c0, float wn, float tres, int pair) {
-  const bool pos = tres >= 0.f;
-  const float lnt = tres > 0.f ? logf(tres) : (tres == 0.f ? -INFINITY : 0.f);
+  const bool pos = tres > 0.f;
+  const float lnt = pos ? logf(tres) : 0.f;
   float4* d = reinterpret_cast<float4*>(r);
   d[0] = make_float4(ct, st, c0, wn);
   d[1] = make_float4(tres, lnt, __int_as_float(pair), __int_as_float(pos ? 1 : 0));
