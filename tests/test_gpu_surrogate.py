@@ -151,6 +151,20 @@ def test_surrogate_trains_and_falls_back_to_mc(propagator):
     mc_rate = 256 / (time.perf_counter() - t0)
     print("queries/s network", nn_rate, "MC", mc_rate)
     assert nn_rate > 1000 * mc_rate
+    # the event likelihood's parameters from the surrogate: module-major, A = mu of the pair,
+    # the time shift = emission time + (d - r) n_g(800 nm) / c
+    from photonprop_b200 import event as ev
+    src = sg.training_pairs(4, 1_000_000, seed=15, d_min=2.0, d_max=10.0)
+    src["emitter"] = pp._lib.EMITTER_CHERENKOV_CONE
+    src["track_len"] = 1.0
+    mods = np.array([[3.0, 1.0, 2.0, 0.21], [-2.0, 4.0, 1.0, 0.21], [1.0, -3.0, 5.0, 0.21]])
+    from photonprop_b200 import lightyield as ly
+    pairs_sm = ly.cross_pairs(propagator, src, mods, seed=3)
+    prm = ev.surrogate_params(s, pairs_sm, len(src), len(mods), propagator.medium)
+    assert prm.shape == (3, 4, 6)
+    mu, _ = s.predict(pairs_sm)
+    np.testing.assert_allclose(prm[:, :, 0], mu[:, 0].reshape(4, 3).T, rtol=1e-12)
+    assert np.all(prm[:, :, 5] > 0)
     # outside the trained distance range the MC kernel answers
     far = sg.training_pairs(4, 200_000, seed=13, d_min=100.0, d_max=120.0)
     out, used_mc = s.predict(far)
