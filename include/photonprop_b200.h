@@ -323,9 +323,10 @@ PP_API pp_status pp_dir_reweight(const double* thetas, double obs_angle, const d
  * where no hit has tres > 0; det_fraction); moments (may be NULL) =
  * n_pairs x n_angles x PP_FIT_MOMENTS; stats / hist as pp_propagate (may be
  * NULL); *n_hits = all hits.  hit_capacity sizes the device hit buffer:
- * pairs run in waves whose hits fit it (a wave that overflows is repacked
- * with the exact per-pair hit counts it produced and run again), so it
- * bounds memory, not the number of hits; PP_ERR_OVERFLOW
+ * pairs run in waves whose hits fit it, planned from a pilot launch of the
+ * first photons of every pair (a wave that overflows is repacked with the
+ * exact per-pair hit counts it produced and run again), so it bounds
+ * memory, not the number of hits; PP_ERR_OVERFLOW
  * only when one pair alone has more hits.  The whole of make_photon_fits
  * (src/modelling.jl:86-111) for all distances is one call. */
 PP_API pp_status pp_propagate_fit(pp_ctx* ctx, const pp_pair* pairs, int64_t n_pairs,

@@ -122,6 +122,7 @@ struct pp_ctx {
   pp::FitConsts fitk;
   DevBuf fit_counts, fit_rec, fit_moments, fit_out, fit_cs;
   DevBuf llh_chunks;  // event likelihood: first hit chunk of every module
+  DevBuf pilot;       // fit waves: the pilot launch's pairs
 
   pp_status fail(pp_status s, const std::string& msg) {
     err = msg;
@@ -204,7 +205,7 @@ void resolve_launch(pp_ctx* c, const pp_run_opts& o, int& grid, int& block, uint
   block = o.block_size > 0 ? o.block_size : c->tuned_block[m];
   if (block != 128) block = 256;  // the batched kernel exists for 4- and 8-warp blocks
   int bps = o.blocks_per_sm > 0 ? o.blocks_per_sm : c->tuned_bps[m];
-  const int maxb = pp::batched_max_blocks_per_sm(m, block);
+  const int maxb = pp::batched_max_blocks_per_sm(m, block, (o.flags & PP_OPT_CASCADE) != 0);
   if (bps <= 0 || bps > maxb) bps = maxb > 0 ? maxb : 1;
   grid = c->sm_count * bps;
   chunk = (uint32_t)(o.chunk_photons > 0 ? o.chunk_photons : c->tuned_chunk[m]);
@@ -466,7 +467,7 @@ void pp_destroy(pp_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     c->drop_graphs();
     for (DevBuf* b : {&c->pairs, &c->hits, &c->counters, &c->stats, &c->hist, &c->offsets, &c->queue, &c->fit_counts,
-                      &c->fit_rec, &c->fit_moments, &c->fit_out, &c->fit_cs, &c->llh_chunks})
+                      &c->fit_rec, &c->fit_moments, &c->fit_out, &c->fit_cs, &c->llh_chunks, &c->pilot})
       b->release();
     if (c->d_tables) cudaFree(c->d_tables);
     if (c->d_casc) cudaFree(c->d_casc);
@@ -812,6 +813,61 @@ static double expected_hits_geo(const pp_pair& q) {
   return f * (double)q.n_photons;
 }
 
+// Per-pair hit estimates for planning waves from a pilot launch: the first
+// min(N, P) photons of every pair, hit records off.  The photons of a pair
+// are a fixed function of (seed, photon index), so these are the full run's
+// first photons; their hit counts h, scaled by N / P with four Poisson
+// standard deviations added, bound the full counts (exact where P = N).  P is
+// 1/64 of the mean photons per pair (at least 65,536); no pilot runs when
+// every photon of the batch fits the buffer (at most one hit per photon) or
+// when the pilot would cost more than 1/8 of the batch (est stays empty).
+static pp_status pilot_estimate(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp_run_opts& o,
+                                int64_t cap, std::vector<double>& est) {
+  est.clear();
+  double photons = 0.0;
+  for (int64_t i = 0; i < n_pairs; ++i) photons += (double)pairs[i].n_photons;
+  if (n_pairs == 0 || photons <= (double)cap) return PP_OK;
+  const int64_t P = std::max<int64_t>(65536, (int64_t)(photons / (64.0 * (double)n_pairs)));
+  std::vector<pp_pair> pilot(pairs, pairs + n_pairs);
+  double pilot_photons = 0.0;
+  for (auto& q : pilot) {
+    q.n_photons = std::min<int64_t>(q.n_photons, P);
+    pilot_photons += (double)q.n_photons;
+  }
+  if (pilot_photons > photons / 8.0) return PP_OK;
+  cudaStream_t s = c->stream;
+  cudaError_t e;
+  bool grew = false;
+  if ((e = ensure(c->pilot, (size_t)n_pairs * sizeof(pp_pair), &grew))) return alloc_fail(c, e, "pilot pairs");
+  pp_run_opts po = o;
+  po.flags |= PP_OPT_NO_HITS;
+  po.hist_bins = 0;
+  pp::LaunchArgs a = base_args(c, &po);
+  a.pairs = static_cast<const pp_pair*>(c->pilot.p);
+  a.n_pairs = n_pairs;
+  a.chunk_offsets = static_cast<unsigned long long*>(c->offsets.p);
+  a.queue = static_cast<unsigned long long*>(c->queue.p);
+  a.hits = static_cast<pp_hit*>(c->hits.p);
+  a.hit_cap = 0;
+  a.counters = static_cast<unsigned long long*>(c->counters.p);
+  a.stats = static_cast<double*>(c->stats.p);
+  a.hist = nullptr;
+  std::vector<double> h(n_pairs);
+  if ((e = cudaMemcpyAsync(c->pilot.p, pilot.data(), (size_t)n_pairs * sizeof(pp_pair), cudaMemcpyHostToDevice,
+                           s)) ||
+      (e = run_batched(c, a, s, false)) ||
+      (e = cudaMemcpy2DAsync(h.data(), sizeof(double), a.stats, PP_STATS * sizeof(double), sizeof(double),
+                             (size_t)n_pairs, cudaMemcpyDeviceToHost, s)) ||
+      (e = cudaStreamSynchronize(s)))
+    return c->cuda_fail(e, "pp_propagate_fit pilot");
+  est.resize(n_pairs);
+  for (int64_t i = 0; i < n_pairs; ++i) {
+    const double n = (double)pairs[i].n_photons, p = (double)pilot[i].n_photons;
+    est[i] = p >= n ? h[i] : (h[i] + 4.0 * std::sqrt(h[i]) + 4.0) * (n / p);
+  }
+  return PP_OK;
+}
+
 pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp_run_opts* opts,
                            const double* obs_angles, int32_t n_angles, int64_t cap, int64_t* n_hits, double* fits,
                            double* moments, double* stats, double* hist) {
@@ -853,13 +909,14 @@ pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, con
        (e = cudaMemsetAsync(d_mom, 0, rows * PP_FIT_MOMENTS * sizeof(double), s))))
     return c->cuda_fail(e, "pp_propagate_fit setup");
   // Waves of pairs whose hits fit the hit buffer: each wave propagates, then
-  // adds its hits' moments.  A pair's hits are estimated from geometry,
-  // scaled by what the waves so far produced; a wave that overflows still
-  // counted every pair's hits exactly (its statistics are complete and the
-  // photons are a fixed function of the seeds), so it is repacked with those
-  // counts and its reruns fit.
-  std::vector<double> geo(n_pairs), exact(n_pairs, -1.0);
+  // adds its hits' moments.  A pair's hits are estimated by a pilot launch
+  // (or, without one, from geometry scaled by what the waves so far
+  // produced); a wave that overflows still counted every pair's hits exactly
+  // (its statistics are complete and the photons are a fixed function of the
+  // seeds), so it is repacked with those counts and its reruns fit.
+  std::vector<double> geo(n_pairs), exact(n_pairs, -1.0), est;
   for (int64_t i = 0; i < n_pairs; ++i) geo[i] = expected_hits_geo(pairs[i]);
+  if ((st = pilot_estimate(c, pairs, n_pairs, o, cap, est))) return st;
   double scale = 4.0;
   int64_t total = 0;
   std::vector<double> wst;
@@ -868,8 +925,8 @@ pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, con
       int64_t to = from;
       double acc = 0.0;
       while (to < n_pairs) {
-        const double w = exact[to] >= 0.0 ? exact[to] : scale * geo[to];
-        if (to > from && acc + w > 0.8 * (double)cap) break;
+        const double w = exact[to] >= 0.0 ? exact[to] : (est.empty() ? scale * geo[to] : est[to]);
+        if (to > from && acc + w > (est.empty() ? 0.8 : 0.95) * (double)cap) break;
         acc += w;
         ++to;
       }
@@ -1040,7 +1097,7 @@ pp_status pp_autotune(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp
   double best = -1.0;
   pp_run_opts bo = *opts;
   for (int b : blocks) {
-    const int maxb = pp::batched_max_blocks_per_sm(m, b);
+    const int maxb = pp::batched_max_blocks_per_sm(m, b, (opts->flags & PP_OPT_CASCADE) != 0);
     for (int bps = 1; bps <= maxb; bps = (bps < maxb && bps * 2 > maxb) ? maxb : bps * 2) {
       for (int ch : chunks) {
         pp_run_opts o = *opts;

@@ -343,9 +343,12 @@ __device__ __forceinline__ EmissionFrame emission_frame(const DevTables& T, cons
     f.oy = dl.y;
     f.oz = dl.z;
     const float c0 = rcp(phase_index(T, rcp(f.wl)));
-    const bool casc = EM == kEmCascade && emitter == PP_EMITTER_CASCADE;
-    f.cpol = casc ? cascade_cos_theta(T, c0, d.u1) : c0;
-    const float s = casc ? 0.f : d.u1 * dl.w;
+    f.cpol = c0;
+    float s = d.u1 * dl.w;
+    if (EM == kEmCascade && emitter == PP_EMITTER_CASCADE) {
+      f.cpol = cascade_cos_theta(T, c0, d.u1);
+      s = 0.f;
+    }
     f.px = fmaf(s, f.ox, f.px);
     f.py = fmaf(s, f.oy, f.py);
     f.pz = fmaf(s, f.oz, f.pz);

@@ -53,7 +53,7 @@ cudaError_t launch_stacks(const LaunchArgs& a, const pp_pair* d_pair, float* pos
 cudaError_t launch_finalize(const pp_pair* pairs, int64_t n, double* stats, double* hist, int bins, int normalize,
                             int sm_count, cudaStream_t s);
 cudaError_t launch_eval(int op, const double* in, double* out, int64_t n, const void* tables, cudaStream_t s);
-int batched_max_blocks_per_sm(int mode, int block);
+int batched_max_blocks_per_sm(int mode, int block, bool cascade);
 int plain_max_blocks_per_sm(int mode, int block);
 cudaError_t run_peaks(int sm_count, double* fp32, double* mufu, double* iops);
 

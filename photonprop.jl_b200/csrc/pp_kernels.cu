@@ -39,8 +39,13 @@ struct __align__(16) Staged {
   uint32_t pad;
 };
 
+// Register budget: 64 per thread (1024 threads per SM) for the basic
+// emitters; the cascade variant's table lookups in the emission block spill
+// at 64, so it gets 80 (768 threads per SM), which runs cone and isotropic
+// pairs as fast as the basic variant does.
 template <int MODE, int WARPS, int EM>
-__global__ void __launch_bounds__(WARPS * 32, 1024 / (WARPS * 32)) batched_kernel(const RunParams R) {
+__global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / (WARPS * 32))
+    batched_kernel(const RunParams R) {
   __shared__ __align__(16) DevTables T;
   __shared__ Staged stage[WARPS][kStage];
   __shared__ WarpStats wstats[WARPS];
@@ -624,16 +629,21 @@ cudaError_t launch_eval(int op, const double* in, double* out, int64_t n, const 
   return cudaGetLastError();
 }
 
-int batched_max_blocks_per_sm(int mode, int block) {
+int batched_max_blocks_per_sm(int mode, int block, bool cascade) {
   int nb = 0;
+  const bool c = mode == PP_MODE_PHYSICAL && cascade;
   if (block == 128) {
     if (mode == PP_MODE_COMPAT)
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kCompat, 4, ppd::kEmBasic>, 128, 0);
+    else if (c)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical, 4, ppd::kEmCascade>, 128, 0);
     else
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical, 4, ppd::kEmBasic>, 128, 0);
   } else {
     if (mode == PP_MODE_COMPAT)
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kCompat, 8, ppd::kEmBasic>, 256, 0);
+    else if (c)
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical, 8, ppd::kEmCascade>, 256, 0);
     else
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, ppd::batched_kernel<ppd::kPhysical, 8, ppd::kEmBasic>, 256, 0);
   }

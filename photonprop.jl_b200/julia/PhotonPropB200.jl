@@ -202,7 +202,7 @@ every (distance, angle) is reweighted and fitted on the device.  Returns a
 NamedTuple of the reference's DataFrame columns.
 """
 function make_photon_fits(ctx::Context, n_photons_per_dist::Integer, n_distances::Integer, n_angles::Integer,
-                          max_dist::Real=300f0; seed::Integer=0, hit_capacity::Integer=1 << 25)
+                          max_dist::Real=300f0; seed::Integer=0, hit_capacity::Integer=1 << 27)
     distances = Float32.(10 .^ sobol_1d(0.0, Float64(Float32(log10(Float32(max_dist)))), n_distances))
     obs_angles = sobol_1d(0.0, Float64(pi), n_angles)
     pairs = [PPPair((0f0, 0f0, 0f0), 0f0, (0f0, 0f0, 1f0), 0f0, (0f0, 0f0, d), 0.21f0, Int64(n_photons_per_dist),

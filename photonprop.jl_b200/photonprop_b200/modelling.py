@@ -131,8 +131,9 @@ def propagate_fit(propagator: Propagator, pairs, obs_angles, opts: RunOptions | 
     """Propagates a batch and fits every (pair, observation angle) on the
     device (pp_propagate_fit).  hit_capacity sizes the device hit buffer
     (96 bytes per hit with the fit records); the library runs the pairs in
-    waves that fit it.  The default is four times the geometric estimate of
-    the hits, between 2^16 and 2^25 (at most 3.2 GB of device memory)."""
+    waves that fit it, planned from a pilot launch of the first photons of
+    every pair.  The default is the batch's photon count (every photon hits
+    at most once), between 2^16 and 2^27 (at most 12.9 GB of device memory)."""
     opts = opts or RunOptions(mode="compat", pmt_weight=True)
     o = opts.to_c()
     o.hist_bins = 0
@@ -140,10 +141,7 @@ def propagate_fit(propagator: Propagator, pairs, obs_angles, opts: RunOptions | 
     angles = np.ascontiguousarray(np.ravel(obs_angles), dtype=np.float64)
     n_p, n_a = len(pairs), len(angles)
     if hit_capacity is None:
-        d = np.linalg.norm(pairs["target"].astype(np.float64) - pairs["pos"].astype(np.float64), axis=1)
-        r = pairs["radius"].astype(np.float64)
-        frac = np.minimum(1.0, r * r / (4.0 * np.maximum(d - r, 1e-3) ** 2))
-        hit_capacity = int(min(max(4 * (frac * pairs["n_photons"]).sum(), 1 << 16), 1 << 25))
+        hit_capacity = int(min(max(int(pairs["n_photons"].sum()), 1 << 16), 1 << 27))
     fits = np.zeros((n_p, n_a, _lib.FIT_OUT))
     mom = np.zeros((n_p, n_a, _lib.FIT_MOMENTS))
     stats = np.zeros((n_p, 8))

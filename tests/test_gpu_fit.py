@@ -139,9 +139,13 @@ def test_make_photon_fits_table(propagator, tmp_path):
     np.testing.assert_array_equal(back.to_numpy(), df.to_numpy())
 
 
-def test_waves_match_one_launch(propagator):
-    pairs = np.concatenate([pp.batches.point_source_pair(1_000_000, target=(0.0, 0.0, 3.0),
-                                                         seed=pp.propagation.pair_seed(11, i)) for i in range(8)])
+@pytest.mark.parametrize("n_photons,n_pairs", [(1_000_000, 8), (60_000, 16)])
+def test_waves_match_one_launch(propagator, n_photons, n_pairs):
+    """Waves planned from the pilot launch's estimates (1e6 photons per pair),
+    and waves planned from geometry alone (pairs too small for a pilot), whose
+    first wave overflows and is repacked with the exact counts."""
+    pairs = np.concatenate([pp.batches.point_source_pair(n_photons, target=(0.0, 0.0, 3.0),
+                                                         seed=pp.propagation.pair_seed(11, i)) for i in range(n_pairs)])
     ro = pp.RunOptions(mode="compat", pmt_weight=True, hist_bins=0)
     one = md.propagate_fit(propagator, pairs, ANGLES, ro, hit_capacity=1 << 21)
     assert one.n_hits < 1 << 21
