@@ -70,6 +70,9 @@ def parse():
     ap.add_argument("--full-weight-hits", type=float, default=1000.0)
     ap.add_argument("--max-photons", type=int, default=0,
                     help="cap photons per pair (small profiling cases; 0 = no cap)")
+    ap.add_argument("--cascade-variant", action="store_true",
+                    help="batch workload: run the kernel variant that samples the cascade profile "
+                         "(PP_OPT_CASCADE) on the same pairs")
     return ap.parse_args()
 
 
@@ -767,7 +770,7 @@ def run_ours(args):
     medium = pp.make_seawater(35.0, 2.0)
     spec = pp.CherenkovSpectrum((300.0, 800.0), 20, medium)
     prop = pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=local)
-    ro = pp.RunOptions(**RUN_KW)
+    ro = pp.RunOptions(**RUN_KW, cascade=args.cascade_variant)
     W, K = args.warmup, args.steps
     batches = [pp.batches.mixed_batch(args.pairs, seed=args.seed + 7919 * rank + i) for i in range(W + K)]
     if args.max_photons > 0:
@@ -949,7 +952,8 @@ def run_ours(args):
                    "mode": "physical", "histogram": "1000 x 1 ns FP64 per pair",
                    "l2": "flushed between steps (256 MiB write, outside the per-step events)",
                    "launch": {"block": ro.block_size, "blocks_per_sm": ro.blocks_per_sm,
-                              "chunk_photons": ro.chunk_photons, "autotuned": tune is not None},
+                              "chunk_photons": ro.chunk_photons, "autotuned": tune is not None,
+                              "kernel_variant": "cascade emitter" if args.cascade_variant else "basic emitters"},
                    "timing": "CUDA events per step on the launch stream, summed; max over ranks",
                    "parallelism": f"{world} independent ranks (weak scaling, no collective)"},
         "latency_ms": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
