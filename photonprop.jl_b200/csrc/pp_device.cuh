@@ -258,35 +258,39 @@ struct RunParams {
   HG hg;
 };
 
-// Registers of one live photon.
+// Registers of one live photon.  The position is kept relative to the
+// target sphere's centre (the ray-sphere test needs nothing else; the hit
+// record adds the centre back), and the path as what the step logic
+// compares: in physical mode the path left before t_max, in compat mode
+// (no time window) the path travelled.
 struct Photon {
-  float px, py, pz;
+  float px, py, pz;   // position - sphere centre
   float dx, dy, dz;
-  float dist;
+  float path;         // physical: path left before t_max; compat: path travelled
   float neg_ln2_len;  // -ln2 * scattering length: step = lg2(u) * this
-  float max_dist;     // physical mode: path length at t_max
   uint32_t ctr3;      // Philox counter word of the next event: block (= steps + 1) << 8 | photon bits 32..39
   uint64_t id;
 };
 
 struct PairCtx {
-  float tx, ty, tz, r;  // sphere centre and radius
+  float r;  // sphere radius
   uint32_t seed_lo, seed_hi;
   int32_t index;
 };
 
 __device__ __forceinline__ PairCtx load_pair_ctx(const pp_pair* __restrict__ P, int index) {
-  const float4 t = __ldg(reinterpret_cast<const float4*>(P) + 2);  // target, radius
-  const uint2 sd = __ldg(reinterpret_cast<const uint2*>(P) + 7);   // seed
+  const uint2 sd = __ldg(reinterpret_cast<const uint2*>(P) + 7);  // seed
   PairCtx c;
-  c.tx = t.x;
-  c.ty = t.y;
-  c.tz = t.z;
-  c.r = t.w;
+  c.r = __ldg(reinterpret_cast<const float*>(P) + 11);  // radius
   c.seed_lo = sd.x;
   c.seed_hi = sd.y;
   c.index = index;
   return c;
+}
+
+__device__ __forceinline__ float3 pair_target(const pp_pair* __restrict__ P) {
+  const float4 t = __ldg(reinterpret_cast<const float4*>(P) + 2);  // target, radius
+  return make_float3(t.x, t.y, t.z);
 }
 
 // Where and how a photon is emitted, from block 0 of its stream
@@ -384,6 +388,13 @@ __device__ __forceinline__ void emission_direction(const EmissionFrame& f, float
   }
 }
 
+// Path a photon emitted in frame f can travel before t_max at the group
+// velocity c / n_g(wl): the emission and the hit record evaluate this one
+// expression, so the hit's path travelled is this minus the path left.
+__device__ __forceinline__ float path_at_tmax(const DevTables& T, const RunParams& R, const EmissionFrame& f) {
+  return (R.t_max - f.t_emit) * kCVac * rcp(group_index(T, rcp(f.wl)));
+}
+
 // Emission of photon s.id (block 0): position, direction and the
 // per-wavelength constants; afterwards the next event is block 1.
 template <int MODE, int EM = kEmBasic>
@@ -391,12 +402,12 @@ __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& 
                                            const PairCtx& c, Photon& s) {
   const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, ctr_word(s.id, 0u));
   const EmissionFrame f = emission_frame<MODE, EM>(T, P, d);
-  s.px = f.px;
-  s.py = f.py;
-  s.pz = f.pz;
-  s.dist = 0.f;
+  const float3 tg = pair_target(P);
+  s.px = f.px - tg.x;
+  s.py = f.py - tg.y;
+  s.pz = f.pz - tg.z;
+  s.path = (MODE == kPhysical) ? path_at_tmax(T, R, f) : 0.f;
   s.neg_ln2_len = -kLn2 * scattering_length(T, f.wl);
-  s.max_dist = (MODE == kPhysical) ? (R.t_max - f.t_emit) * kCVac * rcp(group_index(T, rcp(f.wl))) : 3.0e38f;
   emission_direction(f, d.u2, s.dx, s.dy, s.dz);
   s.ctr3 = ctr_word(s.id, 1u);
 }
@@ -409,7 +420,7 @@ template <int MODE>
 __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c, Photon& s, bool& hit) {
   const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, s.ctr3);
   const float step = lg2(d.u0) * s.neg_ln2_len;
-  const float ex = s.px - c.tx, ey = s.py - c.ty, ez = s.pz - c.tz;
+  const float ex = s.px, ey = s.py, ez = s.pz;  // photon - sphere centre
   const float a = fmaf(s.dz, ez, fmaf(s.dy, ey, s.dx * ex));
   // b = a^2 - |e|^2 + r^2 (src/photon_prop_cuda.jl:340) evaluated as r^2 - |e - a d|^2:
   // the same number, but without cancelling two large squares, which in FP32
@@ -428,20 +439,20 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
     move = !line;  // the line meets the sphere outside this step: no move (reference)
     alive = !geo;
   } else {
-    hit = geo && s.dist + dd <= s.max_dist;  // arrives inside the time window
+    hit = geo && dd <= s.path;  // arrives inside the time window
     // A photon farther from the sphere than the path it has left before t_max
     // can never arrive in time (any path to the sphere is at least the straight
     // distance): it ends now.  Exact, with a margin for FP32 rounding; it
     // spares the steps of photons drifting away from their target.
-    const float reach = fmaf(s.max_dist - s.dist, 1.0001f, c.r + 0.05f);
-    move = !geo && s.dist + step <= s.max_dist && pp <= reach * reach;
+    const float reach = fmaf(s.path, 1.0001f, c.r + 0.05f);
+    move = !geo && step <= s.path && pp <= reach * reach;
     alive = move;
   }
   const float len = hit ? dd : (move ? step : 0.f);
   s.px = fmaf(len, s.dx, s.px);
   s.py = fmaf(len, s.dy, s.py);
   s.pz = fmaf(len, s.dz, s.pz);
-  s.dist += len;
+  s.path += (MODE == kPhysical) ? -len : len;
   const float cpol = hg_costheta(R.hg, d.u1);
   float rx, ry, rz;
   polar_direction(s.dx, s.dy, s.dz, cpol, sin_from_cos(cpol), d.u2, rx, ry, rz);
@@ -468,6 +479,8 @@ __device__ __forceinline__ bool photon_event(const DevTables& T, const RunParams
 struct HitValues {
   float time, weight, wl;
   float d0x, d0y, d0z;
+  float px, py, pz;  // hit position (absolute)
+  float dist;        // path travelled
 };
 
 template <int MODE, int EM = kEmBasic>
@@ -478,13 +491,18 @@ __device__ __forceinline__ HitValues hit_values(const DevTables& T, const RunPar
   HitValues h;
   h.wl = f.wl;
   emission_direction(f, d.u2, h.d0x, h.d0y, h.d0z);
+  const float3 tg = pair_target(P);
+  h.px = s.px + tg.x;
+  h.py = s.py + tg.y;
+  h.pz = s.pz + tg.z;
+  h.dist = (MODE == kPhysical) ? path_at_tmax(T, R, f) - s.path : s.path;
   const float x = 1.f / f.wl;
   if (MODE == kCompat) {
-    h.time = s.dist * phase_index(T, x) / kCVac;  // phase velocity (reference)
+    h.time = h.dist * phase_index(T, x) / kCVac;  // phase velocity (reference)
   } else {
-    h.time = f.t_emit + s.dist * group_index(T, x) / kCVac;
+    h.time = f.t_emit + h.dist * group_index(T, x) / kCVac;
   }
-  float w = expf(-s.dist / interp_sorted(f.wl, T.abs_wl, T.abs_len, T.n_abs));
+  float w = expf(-h.dist / interp_sorted(f.wl, T.abs_wl, T.abs_len, T.n_abs));
   if ((R.flags & PP_OPT_PMT_WEIGHT) && T.n_pmt > 0) w *= interp_sorted(f.wl, T.pmt_wl, T.pmt_acc, T.n_pmt);
   h.weight = w;
   return h;
@@ -506,15 +524,15 @@ __device__ __forceinline__ void write_hit(const RunParams& R, const PairCtx& c, 
   if (idx < R.hit_cap) {
     if (R.flags & PP_OPT_COMPACT_HITS) {
       float4* dst = reinterpret_cast<float4*>(reinterpret_cast<pp_hit32*>(R.hits) + idx);
-      dst[0] = make_float4(s.px, s.py, s.pz, h.time);
+      dst[0] = make_float4(h.px, h.py, h.pz, h.time);
       dst[1] = make_float4(h.weight, h.wl, __uint_as_float((uint32_t)s.id),
                            __uint_as_float((uint32_t)c.index + R.pair_base));
     } else {
       float4* dst = reinterpret_cast<float4*>(R.hits + idx);
-      dst[0] = make_float4(s.px, s.py, s.pz, h.time);
+      dst[0] = make_float4(h.px, h.py, h.pz, h.time);
       dst[1] = make_float4(h.d0x, h.d0y, h.d0z, h.weight);
       dst[2] = make_float4(s.dx, s.dy, s.dz, h.wl);
-      dst[3] = make_float4(s.dist, __uint_as_float((uint32_t)c.index + R.pair_base),
+      dst[3] = make_float4(h.dist, __uint_as_float((uint32_t)c.index + R.pair_base),
                            __uint_as_float((uint32_t)s.id), __uint_as_float((uint32_t)(s.id >> 32)));
     }
   } else {

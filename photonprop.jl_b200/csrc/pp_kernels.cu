@@ -33,7 +33,7 @@ namespace ppd {
 constexpr int kStage = 64;  // >= 2 * 32 - 1 staged emissions per warp (power of two)
 
 struct __align__(16) Staged {
-  float px, py, pz, dx, dy, dz, neg_ln2_len, max_dist;
+  float px, py, pz, dx, dy, dz, neg_ln2_len, path;
   uint32_t id_lo, id_hi;
   int32_t pair;
   uint32_t pad;
@@ -75,10 +75,10 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
   Photon s;
   s.id = 0;
   s.ctr3 = 1u << 8;
-  s.px = s.py = s.pz = s.dx = s.dy = s.dist = s.neg_ln2_len = s.max_dist = 0.f;
+  s.px = s.py = s.pz = s.dx = s.dy = s.path = s.neg_ln2_len = 0.f;
   s.dz = 1.f;
   PairCtx c;
-  c.tx = c.ty = c.tz = c.r = 0.f;
+  c.r = 0.f;
   c.seed_lo = c.seed_hi = 0u;
   c.index = 0;
   unsigned steps = 0;
@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         emit_event<MODE, EM>(T, R, P, pc, e);
         float4* dst = reinterpret_cast<float4*>(ring + ((r_head + r_count + lane) & (kStage - 1)));
         dst[0] = make_float4(e.px, e.py, e.pz, e.dx);
-        dst[1] = make_float4(e.dy, e.dz, e.neg_ln2_len, e.max_dist);
+        dst[1] = make_float4(e.dy, e.dz, e.neg_ln2_len, e.path);
         dst[2] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)),
                              __int_as_float(ppair), 0.f);
       }
@@ -164,8 +164,7 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         s.dy = b.x;
         s.dz = b.y;
         s.neg_ln2_len = b.z;
-        s.max_dist = b.w;
-        s.dist = 0.f;
+        s.path = b.w;
         s.id = ((unsigned long long)__float_as_uint(d.y) << 32) | __float_as_uint(d.x);
         s.ctr3 = ctr_word(s.id, 1u);
         const int pr = __float_as_int(d.z);
@@ -274,14 +273,14 @@ __global__ void __launch_bounds__(1024) stacks_kernel(const RunParams R, const p
         const int idx = atomicAdd(&cursor, 1);  // 1-based slot
         if (idx < ix_offset + stack_len) {
           const int j = idx - 1;
-          out_pos[3 * j + 0] = s.px;
-          out_pos[3 * j + 1] = s.py;
-          out_pos[3 * j + 2] = s.pz;
+          out_pos[3 * j + 0] = h.px;
+          out_pos[3 * j + 1] = h.py;
+          out_pos[3 * j + 2] = h.pz;
           out_dir[3 * j + 0] = h.d0x;
           out_dir[3 * j + 1] = h.d0y;
           out_dir[3 * j + 2] = h.d0z;
           out_wl[j] = h.wl;
-          out_dist[j] = s.dist;
+          out_dist[j] = h.dist;
           atomicMax(out_sp + blockIdx.x, idx);
         } else {
           atomicOr(R.counters + 2, 1ull);

@@ -4,21 +4,23 @@ path (no sphere intersection in the step), physical mode:
 
 per photon step   6 MUFU  (lg2 step length, rcp HG, sqrt sin(theta), sin, cos,
                            rcp rotation)
-                 58 FP32  (FFMA/FMUL/FADD: uniforms 3, step 1, ray-sphere 15
-                           (e, a, e - a d, its square, b, |e|^2, dd), reachability
-                           cut 3, move 4, HG 4, sin(theta) 1, azimuth 3,
-                           rotation with Newton renormalisation 24)
+                 55 FP32  (FFMA/FMUL/FADD: uniforms 3, step 1, ray-sphere 12
+                           (a, e - a d, its square, b, |e|^2, dd; the photon's
+                           position is kept relative to the sphere centre, so e
+                           costs nothing), reachability cut 3, move 4 (position,
+                           path left), HG 4, sin(theta) 1, azimuth 3, rotation
+                           with Newton renormalisation 24)
                   1 Philox4x32-10 block (10 rounds of 2 IMAD.WIDE, 2 LOP3, 2 IADD)
-per photon start  isotropic: 10 MUFU, 25 FP32; Cherenkov cone: 14 MUFU, 57 FP32;
+per photon start  isotropic: 10 MUFU, 28 FP32; Cherenkov cone: 14 MUFU, 60 FP32;
                   plus one Philox block.
 A photon that hits the sphere also re-draws its emission block (rare).
 """
 
 MUFU_PER_STEP = 6
-FP32_PER_STEP = 58
+FP32_PER_STEP = 55
 PHILOX_PER_STEP = 1
 MUFU_PER_PHOTON = {0: 10, 1: 14}   # by emitter type
-FP32_PER_PHOTON = {0: 25, 1: 57}
+FP32_PER_PHOTON = {0: 28, 1: 60}
 PHILOX_PER_PHOTON = 1
 
 
