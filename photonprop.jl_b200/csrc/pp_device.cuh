@@ -196,7 +196,12 @@ __device__ __forceinline__ float cascade_cos_theta(const DevTables& T, float c0,
 }
 
 // cos(theta) of Henyey-Greenstein scattering (src/photon_prop_cuda.jl:31-38)
-// with the launch constants of g folded: 1 - g + 2g u = 1 + g(2u - 1).
+// with the launch constants of g folded: 1 - g + 2g u = 1 + g(2u - 1).  The
+// reference clamps the result to [-1, 1]; for u in (0, 1) the formula leaves
+// that interval by at most a rounding, which sin_from_cos absorbs (it clamps
+// 1 - c^2 at 0) and the rotation's renormalisation removes, so the clamp's
+// two min/max instructions (on the busiest pipe, the integer/compare ALU)
+// are left out of the step.
 struct HG {
   float two_g, one_m_g, a, one_p_g2, inv_2g;
   int iso;
@@ -204,8 +209,7 @@ struct HG {
 __device__ __forceinline__ float hg_costheta(const HG& h, float u) {
   if (h.iso) return fmaf(2.f, u, -1.f);
   const float t = h.a * rcp(fmaf(h.two_g, u, h.one_m_g));
-  const float c = fmaf(-t, t, h.one_p_g2) * h.inv_2g;
-  return fminf(fmaxf(c, -1.f), 1.f);
+  return fmaf(-t, t, h.one_p_g2) * h.inv_2g;
 }
 
 // Rotation that takes e_z to the unit vector o, applied to n (the Rodrigues
@@ -430,7 +434,8 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
   const float b = fmaf(c.r, c.r, -q);
   const float pp = fmaf(a, a, q);  // |e|^2
   // branch-free decisions: the line meets the sphere (b >= 0) at dd ahead
-  const float dd = -a - sqrt_a(fmaxf(b, 0.f));
+  // (b < 0 makes dd NaN, which no decision reads: line is false)
+  const float dd = -a - sqrt_a(b);
   const bool line = b >= 0.f;
   const bool geo = line && dd > 0.f && dd < step;  // reaches the sphere within this step
   bool alive, move;
