@@ -219,6 +219,11 @@ __device__ __forceinline__ float hg_costheta(const HG& h, float u) {
 // conditioned in FP32; o = -e_z maps n to (n_x, -n_y, -n_z) as in the
 // reference.  One MUFU (rcp) instead of the reference's sqrt, 2 divides and
 // rsqrt; the result is renormalised with one Newton step instead of rsqrt.
+// kExactNegZ keeps the reference's result at o = -e_z exactly; a step's
+// turn leaves it out (a photon's direction there is -e_z exactly with
+// probability zero, and either sign of n_x is an equally likely azimuth),
+// which takes a compare and a select off the step's critical path.
+template <bool kExactNegZ = true>
 __device__ __forceinline__ void rotate_to_axis(float ox, float oy, float oz, float nx, float ny,
                                                float nz, float& rx, float& ry, float& rz) {
   const float q = fmaf(ox, ny, -oy * nx);
@@ -231,7 +236,7 @@ __device__ __forceinline__ void rotate_to_axis(float ox, float oy, float oz, flo
   const float y = fmaf(ny, oz, fmaf(oy, nz, ox * t));
   const float z = fmaf(nz, oz, -fmaf(ox, nx, oy * ny));
   // o = -e_z exactly: the formula gives (-n_x, -n_y, -n_z), the reference (n_x, -n_y, -n_z)
-  if (!up && s2 == 0.f) x = nx;
+  if (kExactNegZ && !up && s2 == 0.f) x = nx;
   const float f = fmaf(-0.5f, fmaf(x, x, fmaf(y, y, z * z)), 1.5f);
   rx = x * f;
   ry = y * f;
@@ -368,11 +373,12 @@ __device__ __forceinline__ EmissionFrame emission_frame(const DevTables& T, cons
 // Unit vector at polar cos cpol (sin spol) and azimuth 2 pi u about the axis o
 // (update_direction, src/photon_prop_cuda.jl:223-241).  The azimuth is
 // evaluated as 2 pi u - pi in [-pi, pi) and the sine/cosine negated.
+template <bool kExactNegZ = true>
 __device__ __forceinline__ void polar_direction(float ox, float oy, float oz, float cpol, float spol, float u,
                                                 float& rx, float& ry, float& rz) {
   const float ph = fmaf(kTwoPi, u, -kPi);
   const float nx = -cos_a(ph) * spol, ny = -sin_a(ph) * spol;
-  rotate_to_axis(ox, oy, oz, nx, ny, cpol, rx, ry, rz);
+  rotate_to_axis<kExactNegZ>(ox, oy, oz, nx, ny, cpol, rx, ry, rz);
 }
 
 __device__ __forceinline__ float sin_from_cos(float c) { return sqrt_a(fmaxf(0.f, fmaf(-c, c, 1.f))); }
@@ -460,7 +466,7 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
   s.path += (MODE == kPhysical) ? -len : len;
   const float cpol = hg_costheta(R.hg, d.u1);
   float rx, ry, rz;
-  polar_direction(s.dx, s.dy, s.dz, cpol, sin_from_cos(cpol), d.u2, rx, ry, rz);
+  polar_direction<false>(s.dx, s.dy, s.dz, cpol, sin_from_cos(cpol), d.u2, rx, ry, rz);
   s.dx = move ? rx : s.dx;
   s.dy = move ? ry : s.dy;
   s.dz = move ? rz : s.dz;
