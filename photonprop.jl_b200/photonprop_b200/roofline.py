@@ -34,11 +34,11 @@ def op_counts(steps, photons_iso, photons_cone):
 
 # DRAM traffic of the batched kernel per photon, measured with ncu
 # (dram__bytes_read.sum + dram__bytes_write.sum) on one launch of 2.524e8
-# photons (512 mixed pairs, <= 1e6 photons each): 118.0 KB read, 0 B written.
+# photons (512 mixed pairs, <= 1e6 photons each): 117.8 KB read, 0 B written.
 # Hit records and FP64 histogram reductions stay in L2 during a launch, so
 # the traffic grows with the photon count; bench.py scales it to its launch.
-NCU_DRAM_BYTES_PER_PHOTON = 118.016e3 / 252387747
+NCU_DRAM_BYTES_PER_PHOTON = 117.76e3 / 252387747
 # Issue slots busy in the same capture (smsp__issue_active).
-NCU_ISSUE_ACTIVE = 0.778
-NCU_PIPES = {"alu": 0.510, "fma": 0.337, "xu": 0.283}  # pipe utilisation, same capture
+NCU_ISSUE_ACTIVE = 0.775
+NCU_PIPES = {"alu": 0.503, "fma": 0.338, "xu": 0.284}  # pipe utilisation, same capture
 NCU_BRANCH_UNIFORM = 0.914  # smsp__sass_average_branch_targets_threads_uniform, same capture
