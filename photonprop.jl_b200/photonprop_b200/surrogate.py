@@ -211,6 +211,47 @@ def training_pairs(n_pairs, photons, seed=0, d_min=2.0, d_max=150.0, distance_la
     return b
 
 
+# ---- trained-network files (the reference keeps its network in
+# photon_model.bson, example_full.jl:175-178) ------------------------------
+WEIGHTS_MAGIC = b"PPSURR01"
+
+
+def write_weights(path, params, norm18, lo, hi):
+    """Writes a trained network: the magic, int32 version 1, int32 parameter
+    count, int32 inputs (4), int32 outputs (5), then little-endian FP32 arrays:
+    the trained feature range lo[4], hi[4], the normalisation (x mean[4],
+    x std[4], y mean[5], y std[5]) and the parameters in pp_mlp_get_params
+    order."""
+    params = np.ascontiguousarray(params, dtype="<f4").ravel()
+    norm18 = np.ascontiguousarray(norm18, dtype="<f4").ravel()
+    lo = np.ascontiguousarray(lo, dtype="<f4").ravel()
+    hi = np.ascontiguousarray(hi, dtype="<f4").ravel()
+    if norm18.size != 18 or lo.size != 4 or hi.size != 4:
+        raise ValueError("need 18 normalisation values and a 4-feature range")
+    with open(path, "wb") as f:
+        f.write(WEIGHTS_MAGIC)
+        f.write(np.array([1, params.size, 4, N_OUT], dtype="<i4").tobytes())
+        for arr in (lo, hi, norm18, params):
+            f.write(arr.tobytes())
+
+
+def read_weights(path, n_params=None):
+    """(params, norm18, lo, hi) of a file written by write_weights; ValueError
+    for anything else (wrong magic or version, sizes that do not match the
+    file or, when given, n_params)."""
+    with open(path, "rb") as f:
+        blob = f.read()
+    if len(blob) < 24 or blob[:8] != WEIGHTS_MAGIC:
+        raise ValueError(f"{path}: not a surrogate weights file")
+    version, n, n_in, n_out = np.frombuffer(blob, dtype="<i4", count=4, offset=8).tolist()
+    if version != 1 or n_in != 4 or n_out != N_OUT or n < 1 or (n_params is not None and n != n_params):
+        raise ValueError(f"{path}: version {version}, {n} parameters, {n_in} -> {n_out} does not fit this network")
+    if len(blob) != 24 + 4 * (26 + n):
+        raise ValueError(f"{path}: {len(blob)} bytes, expected {24 + 4 * (26 + n)}")
+    v = np.frombuffer(blob, dtype="<f4", offset=24).astype(np.float32)
+    return v[26:].copy(), v[8:26].copy(), v[0:4].copy(), v[4:8].copy()
+
+
 class Surrogate:
     """Trained network + its feature range; predict() answers queries inside
     the range with the network and the rest with the MC kernel."""
@@ -220,6 +261,24 @@ class Surrogate:
         self.net = MLP(device, seed)
         self.lo = None
         self.hi = None
+
+    def save(self, path):
+        """Writes the trained network and its feature range (write_weights)."""
+        if self.lo is None:
+            raise ValueError("the surrogate is not trained")
+        xm, xs, ym, ys = self.net.get_normalization()
+        write_weights(path, self.net.get_params(), np.concatenate([xm, xs, ym, ys]), self.lo, self.hi)
+
+    @classmethod
+    def load(cls, prop: Propagator, opts: RunOptions, path, device=0):
+        """A surrogate with the network of a file written by save(): the same
+        answers as the network that was saved, without training."""
+        s = cls(prop, opts, device=device)
+        params, norm, lo, hi = read_weights(path, s.net.n_params)
+        s.net.set_params(params)
+        s.net.set_normalization(norm[0:4], norm[4:8], norm[8:13], norm[13:18])
+        s.lo, s.hi = lo.astype(np.float64), hi.astype(np.float64)
+        return s
 
     def fit(self, data: Dataset, epochs=60, batch=4096, lr=1e-3, seed=0, log=None, lr_min=1e-5):
         """Adam with a cosine learning-rate decay from lr to lr_min."""

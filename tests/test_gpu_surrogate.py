@@ -107,7 +107,7 @@ def test_gamma_mixture_fit_recovers_parameters():
     np.testing.assert_allclose(o[:4], [w, a1, a2, th], rtol=0.05)
 
 
-def test_surrogate_trains_and_falls_back_to_mc(propagator):
+def test_surrogate_trains_and_falls_back_to_mc(propagator, tmp_path):
     opts = pp.RunOptions(mode="physical", t_max=1000.0, hist_bins=1000)
     train = sg.mc_dataset(propagator, sg.training_pairs(16384, 1_000_000, seed=11, d_min=2.0, d_max=10.0), opts)
     test = sg.mc_dataset(propagator, sg.training_pairs(1024, 1_000_000, seed=12, d_min=2.0, d_max=10.0), opts)
@@ -165,6 +165,12 @@ def test_surrogate_trains_and_falls_back_to_mc(propagator):
     mu, _ = s.predict(pairs_sm)
     np.testing.assert_allclose(prm[:, :, 0], mu[:, 0].reshape(4, 3).T, rtol=1e-12)
     assert np.all(prm[:, :, 5] > 0)
+    # a saved network, loaded without training, answers the same
+    f = tmp_path / "surrogate.bin"
+    s.save(f)
+    s2 = sg.Surrogate.load(propagator, opts, f)
+    np.testing.assert_array_equal(s2.predict_features(test.x, physical=True), s.predict_features(test.x, physical=True))
+    np.testing.assert_array_equal(s2.in_range(test.x), s.in_range(test.x))
     # outside the trained distance range the MC kernel answers
     far = sg.training_pairs(4, 200_000, seed=13, d_min=100.0, d_max=120.0)
     out, used_mc = s.predict(far)
