@@ -494,6 +494,7 @@ pp_status pp_get_knots(const pp_ctx* c, float* out, int32_t cap, int32_t* n) {
 pp_status pp_propagate_device(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs, const pp_run_opts* opts,
                               pp_hit* d_hits, int64_t cap, uint64_t* d_counters, double* d_stats,
                               double* d_hist, void* stream) {
+  pp::Range range_("pp_propagate_device");
   if (!c) return PP_ERR_ARG;
   std::lock_guard<std::mutex> lk(c->mu);
   pp_status st = validate_opts(c, opts);
@@ -527,6 +528,7 @@ pp_status pp_propagate_device(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs
 
 pp_status pp_propagate(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp_run_opts* opts, pp_hit* hits,
                        int64_t cap, int64_t* n_hits, double* stats, double* hist) {
+  pp::Range range_("pp_propagate");
   if (!c) return PP_ERR_ARG;
   std::lock_guard<std::mutex> lk(c->mu);
   pp_status st = validate_opts(c, opts);
@@ -631,6 +633,7 @@ pp_status pp_propagate_plain_device(pp_ctx* c, const pp_pair* d_pair, const pp_p
 
 pp_status pp_propagate_plain(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp_run_opts* opts,
                              pp_hit* hits, int64_t cap, int64_t* n_hits, double* stats, double* hist) {
+  pp::Range range_("pp_propagate_plain");
   if (!c) return PP_ERR_ARG;
   pp_run_opts o_plain;
   {
@@ -699,6 +702,7 @@ pp_status pp_propagate_plain(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, c
 pp_status pp_cuda_propagate_photons(pp_ctx* c, float* pos, float* dir, float* wl, float* dist, int32_t* sp,
                                     int64_t* nsim, int32_t stack_len, int32_t n_blocks, int32_t threads,
                                     const pp_pair* st_pair, const pp_run_opts* opts, void* stream) {
+  pp::Range range_("pp_cuda_propagate_photons");
   if (!c) return PP_ERR_ARG;
   std::lock_guard<std::mutex> lk(c->mu);
   pp_status st = validate_opts(c, opts);
@@ -823,6 +827,7 @@ static double expected_hits_geo(const pp_pair& q) {
 // when the pilot would cost more than 1/8 of the batch (est stays empty).
 static pp_status pilot_estimate(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp_run_opts& o,
                                 int64_t cap, std::vector<double>& est) {
+  pp::Range range_("pp_propagate_fit pilot");
   est.clear();
   double photons = 0.0;
   for (int64_t i = 0; i < n_pairs; ++i) photons += (double)pairs[i].n_photons;
@@ -871,6 +876,7 @@ static pp_status pilot_estimate(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs
 pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp_run_opts* opts,
                            const double* obs_angles, int32_t n_angles, int64_t cap, int64_t* n_hits, double* fits,
                            double* moments, double* stats, double* hist) {
+  pp::Range range_("pp_propagate_fit");
   if (!c) return PP_ERR_ARG;
   std::lock_guard<std::mutex> lk(c->mu);
   pp_status st = validate_opts(c, opts);
@@ -934,6 +940,7 @@ pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, con
     };
     int64_t end = pick(start);
     unsigned long long cnt[4];
+    pp::Range wave_range("pp_propagate_fit wave");
     for (;;) {
       pp::LaunchArgs a = base_args(c, &o);
       a.pairs = d_pairs + start;
@@ -996,6 +1003,7 @@ pp_status pp_propagate_fit(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, con
 pp_status pp_fit_hits_device(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs, int32_t mode, const pp_hit* d_hits,
                              int64_t cap, const uint64_t* d_counters, const double* obs_angles, int32_t n_angles,
                              double* d_moments, double* d_fits, void* stream) {
+  pp::Range range_("pp_fit_hits_device");
   if (!c) return PP_ERR_ARG;
   std::lock_guard<std::mutex> lk(c->mu);
   if (mode != PP_MODE_COMPAT && mode != PP_MODE_PHYSICAL) return c->fail(PP_ERR_ARG, "unknown mode");
@@ -1052,6 +1060,7 @@ pp_status pp_measure_peaks(int device, double* fp32, double* mufu, double* iops)
 // per (device name, mode): "name|mode|block|blocks_per_sm|chunk|photons_per_s".
 pp_status pp_autotune(pp_ctx* c, const pp_pair* pairs, int64_t n_pairs, const pp_run_opts* opts,
                       const char* cache_path, pp_run_opts* best_out, double* best_rate) {
+  pp::Range range_("pp_autotune");
   if (!c) return PP_ERR_ARG;
   pp_status st;
   {

@@ -181,6 +181,7 @@ extern "C" pp_status pp_event_llh_device(pp_ctx* c, int32_t mode, int64_t n_hyp,
                                          int64_t n_modules, const double* d_params, const double* d_photons,
                                          const int64_t* d_offsets, const double* d_times, double* d_llh,
                                          void* stream) {
+  pp::Range range_("pp_event_llh_device");
   if (!c) return PP_ERR_ARG;
   std::lock_guard<std::mutex> lk(pp::ctx_mutex(c));
   if (mode != PP_LLH_REFERENCE && mode != PP_LLH_SHIFTED) return pp::ctx_fail(c, PP_ERR_ARG, "unknown llh mode");

@@ -3,6 +3,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdint>
@@ -12,6 +13,15 @@
 #include "photonprop_b200.h"
 
 namespace pp {
+
+// Named host-side range for profilers (NVTX, header only: without a
+// profiler attached a push/pop pair is a check of one pointer).
+struct Range {
+  explicit Range(const char* name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range&) = delete;
+  Range& operator=(const Range&) = delete;
+};
 
 // Everything one launch of the propagation kernels reads or writes.
 struct LaunchArgs {

@@ -901,6 +901,7 @@ pp_status pp_mlp_get_normalization(pp_mlp* m, float* out18) {
 }
 
 pp_status pp_mlp_forward(pp_mlp* m, const float* d_x, float* d_out, int64_t n, int32_t physical, void* stream) {
+  pp::Range range_("pp_mlp_forward");
   if (!m || n < 0 || (n > 0 && (!d_x || !d_out))) return PP_ERR_ARG;
   if (n == 0) return PP_OK;
   std::lock_guard<std::mutex> lk(m->mu);
@@ -917,6 +918,7 @@ pp_status pp_mlp_forward(pp_mlp* m, const float* d_x, float* d_out, int64_t n, i
 // One Adam step on a batch (or, with lr = 0 and grad_out, the raw gradients).
 pp_status pp_mlp_train_step(pp_mlp* m, const float* d_xn, const float* d_yt, const float* d_mask, int64_t n,
                             float lr, float* loss_out, float* grad_out) {
+  pp::Range range_("pp_mlp_train_step");
   if (!m || n <= 0 || !d_xn || !d_yt || !d_mask) return PP_ERR_ARG;
   std::lock_guard<std::mutex> lk(m->mu);
   Guard g(m->device);

@@ -214,6 +214,7 @@ void finish_slot(pp_server* S, Slot& s) {
 
 // Packs the head of the queue into slot s and launches it (server lock held).
 bool launch_slot(pp_server* S, Slot& s) {
+  pp::Range range_("pp_server batch launch");
   std::vector<ReqPtr> take;
   int64_t pairs = 0, cap = 0, reserve = 0;
   while (!S->waiting.empty()) {
