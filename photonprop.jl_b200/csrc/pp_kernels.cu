@@ -28,7 +28,7 @@ namespace ppd {
 // its dead lanes outnumber the staged photons, all 32 lanes take the next
 // photon indices from the warp's chunk (grabbing chunks from the device work
 // queue) and compute 32 emissions together, converged; dead lanes then pick
-// staged photons up with three 16-byte loads.  The step loop that follows
+// staged photons up with four 16-byte loads.  The step loop that follows
 // is the same straight-line code for every lane.
 constexpr int kStage = 64;  // >= 2 * 32 - 1 staged emissions per warp (power of two)
 
@@ -36,7 +36,9 @@ struct __align__(16) Staged {
   float px, py, pz, dx, dy, dz, neg_ln2_len, path;
   uint32_t id_lo, id_hi;
   int32_t pair;
-  uint32_t pad;
+  float radius;              // the pair's sphere radius and seed, so that a
+  uint32_t seed_lo, seed_hi;  // refill reads shared memory only
+  uint32_t pad[2];
 };
 
 // Compat mode hits often: a photon whose line meets the sphere beyond its
@@ -184,7 +186,8 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         dst[0] = make_float4(e.px, e.py, e.pz, e.dx);
         dst[1] = make_float4(e.dy, e.dz, e.neg_ln2_len, e.path);
         dst[2] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)),
-                             __int_as_float(ppair), 0.f);
+                             __int_as_float(ppair), pc.r);
+        dst[3] = make_float4(__uint_as_float(pc.seed_lo), __uint_as_float(pc.seed_hi), 0.f, 0.f);
       }
       r_count += filled;
       __syncwarp();
@@ -193,7 +196,7 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
       const unsigned rank = __popc(need & lt_mask);
       if (rank < r_count) {
         const float4* src = reinterpret_cast<const float4*>(ring + ((r_head + rank) & (kStage - 1)));
-        const float4 a = src[0], b = src[1], d = src[2];
+        const float4 a = src[0], b = src[1], d = src[2], e = src[3];
         s.px = a.x;
         s.py = a.y;
         s.pz = a.z;
@@ -204,8 +207,10 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         s.path = b.w;
         s.id = ((unsigned long long)__float_as_uint(d.y) << 32) | __float_as_uint(d.x);
         s.ctr3 = ctr_word(s.id, 1u);
-        const int pr = __float_as_int(d.z);
-        c = load_pair_ctx(R.pairs + pr, pr);
+        c.index = __float_as_int(d.z);
+        c.r = d.w;
+        c.seed_lo = __float_as_uint(e.x);
+        c.seed_hi = __float_as_uint(e.y);
         alive = true;
       }
     }
@@ -213,7 +218,7 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
     r_head += took;
     r_count -= took;
     __syncwarp();
-    if (__ballot_sync(kFull, alive) == 0u) break;
+    if (need == kFull && took == 0u) break;  // every lane was idle and none took a photon
     bool hit = false;
     if (alive) {
       ++steps;
