@@ -101,6 +101,9 @@ def test_default_opts():
     assert o.g == pytest.approx(0.95) and o.t_max == 500.0
     o = pp.RunOptions(mode="physical", pmt_weight=False, normalize=True, write_hits=False, g=0.5).to_c()
     assert o.flags == 2 | 4 and o.g == pytest.approx(0.5)
+    # the cascade-emitter kernel variant is a flag the device entry points take from the caller
+    o = pp.RunOptions(mode="physical", cascade=True, block_size=128, blocks_per_sm=6, chunk_photons=4096).to_c()
+    assert o.flags == 1 | 16 and (o.block_size, o.blocks_per_sm, o.chunk_photons) == (128, 6, 4096)
     with pytest.raises(ValueError):
         pp.RunOptions(mode="nope").to_c()
 
