@@ -205,3 +205,28 @@ def test_oracle_thread_count_invariance():
     assert a[4] == b[4] and a[3] == b[3]
     np.testing.assert_array_equal(a[0], b[0])
     np.testing.assert_array_equal(a[1], b[1])
+
+
+def test_oracle_empty_zero_photon_and_limited_pairs():
+    """Edge cases the kernels are held to: pairs without photons add nothing
+    and keep their rows zero; a photon limit replays exactly the first
+    photons of each pair (the pilot launch of the fit stage relies on this)."""
+    T = _golden_tables()
+    o = O.make_opts(mode=O.MODE_PHYSICAL, g=0.9, t_max=300.0, hist_bins=300)
+    h, s, hist, steps, total = O.propagate(T, O.pairs_array(0), o, n_threads=2)
+    assert total == 0 and steps == 0 and len(h) == 0
+    p = O.pairs_array(3)
+    p["target"] = [(0.0, 0.0, 2.0), (0.0, 0.0, 2.0), (0.0, 2.5, 0.0)]
+    p["radius"] = 0.21
+    p["n_photons"] = [0, 4000, 3000]
+    p["seed"] = [5, 6, 7]
+    h, s, hist, steps, total = O.propagate(T, p, o, n_threads=2)
+    assert total > 0 and not np.any(h["pair"] == 0)
+    assert np.all(s[0] == 0.0) and np.all(hist[0] == 0.0)
+    np.testing.assert_array_equal(s[:, 0], [np.sum(h["pair"] == k) for k in range(3)])
+    hl, sl, _, _, total_l = O.propagate(T, p, o, photon_limit=1500, n_threads=2)
+    full = h[h["photon"] < 1500]
+    assert total_l == len(full)
+    key = lambda a: np.lexsort((a["photon"], a["pair"]))  # noqa: E731
+    np.testing.assert_array_equal(hl[key(hl)]["photon"], full[key(full)]["photon"])
+    np.testing.assert_array_equal(hl[key(hl)]["pos"], full[key(full)]["pos"])
