@@ -146,35 +146,70 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(batch, target_seconds, run_kw):
-    """The FP64 CPU restatement of the reference kernel (oracle/, all host
-    threads) on a bounded sample of the same batch: the first L photons of
-    every pair, L chosen for about target_seconds of work."""
-    from oracle import oracle as O
-    from oracle import tables as tb
-    import photonprop_b200 as pp
-    m = tb.cascadia(35.0, 2.0)
-    knots = tb.cherenkov_spectrum_knots((300.0, 800.0), 20, m)
-    T = O.make_tables(m, knots, pmt=(pp.p_one_pmt_acc.wavelengths, pp.p_one_pmt_acc.acceptance))
-    op = O.pairs_array(len(batch))
-    for f in ("pos", "t0", "dir", "track_len", "target", "radius", "n_photons", "seed", "emitter"):
-        op[f] = batch[f]
-    oo = O.make_opts(mode=O.MODE_PHYSICAL, g=run_kw["g"], t_max=run_kw["t_max"], hist_bins=run_kw["hist_bins"],
-                     flags=O.OPT_PMT_WEIGHT)
-    cores = os.cpu_count() or 1
-    n = np.asarray(batch["n_photons"], dtype=np.int64)
-    lim = 64
-    t0 = time.perf_counter()
-    O.propagate(T, op, oo, photon_limit=lim, n_threads=cores)
-    dt = max(time.perf_counter() - t0, 1e-3)
-    lim = int(max(64, min(n.max(), lim * target_seconds / dt)))
-    t0 = time.perf_counter()
-    O.propagate(T, op, oo, photon_limit=lim, n_threads=cores)
-    dt = time.perf_counter() - t0
-    photons = int(np.minimum(n, lim).sum())
-    return {"value": photons / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"first {lim} photons of each of the {len(batch)} pairs ({photons:.3e} photons, "
-                      f"{dt:.1f} s), FP64 oracle, OpenMP {cores} threads"}
+class CpuArm:
+    """The reference's algorithm on the host cores: the FP64 C restatement of
+    cuda_propagate_photons! (src/photon_prop_cuda.jl:262-386) and of
+    propagate_distance's host finish (:588-644) in oracle/, OpenMP over one
+    flat (pair, photon-chunk) index space on every host thread.  The batch is
+    built by oracle/batches.py (the same numbers as the product's generator),
+    so a process that times it never loads the product library.  The sample is
+    the first ceil(f N_i) photons of every pair, f chosen for a given length of
+    work, so its photon mix (emitters, distances, photons per pair) follows the
+    batch's."""
+
+    def __init__(self, seed, n_pairs, run_kw):
+        from oracle import batches as ob
+        from oracle import oracle as O
+        from oracle import tables as tb
+        self.ob, self.O = ob, O
+        m = tb.cascadia(35.0, 2.0)
+        knots = tb.cherenkov_spectrum_knots((300.0, 800.0), 20, m).astype(np.float32).astype(np.float64)
+        self.T = O.make_tables(m, knots, pmt=ob.pmt_table())
+        self.n_pairs = n_pairs
+        self.batch = ob.mixed_batch(n_pairs, seed=seed)
+        self.oo = O.make_opts(mode=O.MODE_PHYSICAL, g=float(np.float32(run_kw["g"])), t_max=run_kw["t_max"],
+                              hist_t0=run_kw["hist_t0"], hist_bin_width=run_kw["hist_bin_width"],
+                              hist_bins=run_kw["hist_bins"], flags=O.OPT_PMT_WEIGHT)
+        self.cores = os.cpu_count() or 1
+        self.batch_photons = int(self.batch["n_photons"].sum())
+        self.frac = min(1.0, 2e5 / self.batch_photons)
+        self.sample = self.ob.sampled(self.batch, self.frac)
+
+    def run(self):
+        """One pass over the sample: (photons, seconds, threads that ran)."""
+        t0 = time.perf_counter()
+        self.O.propagate(self.T, self.sample, self.oo, n_threads=self.cores)
+        dt = time.perf_counter() - t0
+        return int(self.sample["n_photons"].sum()), dt, self.O.last_threads_used
+
+    def calibrate(self, seconds):
+        """Sizes the sample for about `seconds` of work per pass."""
+        _, dt, _ = self.run()
+        self.frac = min(1.0, self.frac * seconds / max(dt, 1e-3))
+        self.sample = self.ob.sampled(self.batch, self.frac)
+
+    def describe(self, photons, dt, used):
+        return {"value": photons / dt, "unit": UNIT, "cores": used, "kind": "port", "seconds": dt,
+                "photons": photons, "batch_photons": self.batch_photons,
+                "sample": f"first ceil({self.frac:.3e} N_i) photons of each of the {self.n_pairs} pairs of the "
+                          f"batch ({photons:.3e} photons, {dt:.1f} s), FP64 oracle, OpenMP over (pair, photon) "
+                          f"chunks, {used} threads ran (host has {self.cores})"}
+
+
+def cpu_baseline(seed, n_pairs, target_seconds, run_kw):
+    """One calibrated CPU pass of about target_seconds (see CpuArm)."""
+    arm = CpuArm(seed, n_pairs, run_kw)
+    arm.calibrate(target_seconds)
+    return arm.describe(*arm.run())
+
+
+def bench_config(n_pairs, seed, photons, world):
+    """The `config` object both arms print (the same workload)."""
+    return {"workload": WORKLOAD, "pairs": n_pairs, "batch_seed": seed, "photons_per_step_per_gpu": photons,
+            "mode": "physical", "histogram": "1000 x 1 ns FP64 per pair",
+            "l2": "inputs and outputs of a step exceed L2 (~5.9e9 photons, 32.8 MB histograms); the GPU arm "
+                  "also writes 256 MiB between timed steps",
+            "parallelism": f"{world} independent ranks (weak scaling, no collective)"}
 
 
 def run_serving(prop, seconds, seed=0, rate_hz=200.0):
@@ -709,30 +744,39 @@ def run_llh(args):
 
 
 def run_reference(args):
+    """--impl reference: the reference's algorithm (its FP64 C restatement,
+    oracle/) on all host cores, on a bounded sample of the first timed batch of
+    the GPU arm; rank 0 alone runs it.  Nothing here imports the product."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    import photonprop_b200 as pp
     steps, warm = args.steps, args.warmup
-    batch = pp.batches.mixed_batch(args.pairs, seed=args.seed)
-    per_step = max(2.0, min(args.cpu_seconds, 60.0 / max(steps + warm, 1)))
-    vals = []
-    base = None
+    seed = args.seed + warm  # the GPU arm's first timed batch (rank 0)
+    arm = CpuArm(seed, args.pairs, RUN_KW)
+    per_step = max(1.0, min(args.cpu_seconds, 90.0 / max(steps + warm, 1)))
+    arm.calibrate(per_step)
+    photons = []
+    times = []
+    threads = []
     for i in range(warm + steps):
-        b = cpu_baseline(batch, per_step, RUN_KW)
+        ph, dt, used = arm.run()
         if i >= warm:
-            vals.append(b["value"])
-            base = b
-    v = statistics.median(vals)
+            photons.append(ph)
+            times.append(dt)
+            threads.append(used)
+    t = sum(times)
+    v = sum(photons) / t
+    base = arm.describe(photons[-1], statistics.median(times), min(threads))
     base["value"] = v
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-            "steps": steps, "warmup": warm, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "pairs": args.pairs, "sampled": True},
+            "steps": steps, "warmup": warm, "ms_per_step": t * 1e3 / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": bench_config(args.pairs, seed, arm.batch_photons, args.gpus),
             "cpu_baseline": base, "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0,
                                           "d2h_bytes_per_step": 0},
+            "step": "one pass over the sample (the first ceil(f N_i) photons of every pair of the batch)",
             "note": "the reference's propagation exists only as a CUDA.jl kernel (Julia is not installed); "
-                    "this arm times its FP64 C restatement on the host cores"}
+                    "this arm times its FP64 C restatement on the host cores, without the product library"}
     print(json.dumps(line), flush=True)
 
 
@@ -941,21 +985,24 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(batches[W], args.cpu_seconds, RUN_KW)
+        cpu = cpu_baseline(args.seed + W, n_pairs, args.cpu_seconds, RUN_KW)
+        from oracle import batches as ob
+        ob_batch = ob.mixed_batch(n_pairs, seed=args.seed + W)
+        cpu["same_batch_as_gpu"] = bool(np.array_equal(ob_batch["n_photons"], batches[W]["n_photons"])
+                                        and np.array_equal(ob_batch["seed"], batches[W]["seed"])
+                                        and np.array_equal(ob_batch["target"], batches[W]["target"]))
 
     lat = sorted(step_ms)
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": reduce(t_local, MAX) * 1e3 / K, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "pairs": n_pairs, "photons_per_step_per_gpu": photons_local[0],
-                   "mode": "physical", "histogram": "1000 x 1 ns FP64 per pair",
-                   "l2": "flushed between steps (256 MiB write, outside the per-step events)",
-                   "launch": {"block": ro.block_size, "blocks_per_sm": ro.blocks_per_sm,
-                              "chunk_photons": ro.chunk_photons, "autotuned": tune is not None,
-                              "kernel_variant": "cascade emitter" if args.cascade_variant else "basic emitters"},
-                   "timing": "CUDA events per step on the launch stream, summed; max over ranks",
-                   "parallelism": f"{world} independent ranks (weak scaling, no collective)"},
+        "config": bench_config(n_pairs, args.seed + 7919 * rank + W, photons_local[0], world),
+        "launch": {"block": ro.block_size, "blocks_per_sm": ro.blocks_per_sm, "chunk_photons": ro.chunk_photons,
+                   "autotuned": tune is not None,
+                   "kernel_variant": "cascade emitter" if args.cascade_variant else "basic emitters"},
+        "timing": "CUDA events per step on the launch stream, summed; max over ranks; L2 flushed between steps "
+                  "(256 MiB write outside the per-step events)",
         "latency_ms": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
                        "what": "device time of one 4096-pair batch solve"},
         "roofline": {"bound": "mufu", "achieved": a_mufu / 1e9, "peak": peaks["mufu_ops"] / 1e9,

@@ -56,6 +56,7 @@ class Opts(ctypes.Structure):
 
 
 _lib = None
+last_threads_used = 0  # OpenMP team size of the last propagate() call
 
 
 def build(force=False):
@@ -91,7 +92,7 @@ def lib():
         L.orc_propagate.argtypes = [
             ctypes.POINTER(Tables), ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(Opts),
             ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p,
-            ctypes.c_int, ctypes.POINTER(ctypes.c_int64)]
+            ctypes.c_int, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int)]
         L.orc_propagate.restype = ctypes.c_int64
         L.orc_simulate_one.argtypes = [ctypes.POINTER(Tables), ctypes.c_void_p, ctypes.c_int64,
                                        ctypes.c_int64, ctypes.POINTER(Opts), ctypes.c_void_p]
@@ -198,10 +199,13 @@ def propagate(tables: Tables, pairs, opts: Opts, photon_limit=-1, n_threads=0,
     stats = np.zeros((n, N_STATS))
     hist = np.zeros((n, max(opts.hist_bins, 1)))
     steps = ctypes.c_int64(0)
+    used = ctypes.c_int(0)
     total = lib().orc_propagate(
         ctypes.byref(tables), pairs.ctypes.data, n, ctypes.byref(opts), int(photon_limit),
         hits.ctypes.data, hit_cap, stats.ctypes.data, hist.ctypes.data, int(n_threads),
-        ctypes.byref(steps))
+        ctypes.byref(steps), ctypes.byref(used))
+    global last_threads_used
+    last_threads_used = used.value
     return hits[:min(total, hit_cap)], stats, hist[:, :opts.hist_bins], steps.value, total
 
 

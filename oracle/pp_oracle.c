@@ -310,28 +310,58 @@ static int cmp_hit(const void* a, const void* b) {
   return 0;
 }
 
+/* Work items of the flat (pair, photon) index space: chunks of ORC_CHUNK
+ * photons of one pair, so every host thread has work at any photon count. */
+#define ORC_CHUNK 256
+
 int64_t orc_propagate(const orc_tables* t, const orc_pair* pairs, int64_t n_pairs, const orc_opts* o,
                       int64_t photon_limit, orc_hit* hits, int64_t hit_cap, double* stats, double* hist,
-                      int n_threads, int64_t* steps_out) {
+                      int n_threads, int64_t* steps_out, int* threads_used) {
   int nt = n_threads > 0 ? n_threads : 1;
 #ifdef _OPENMP
   if (n_threads <= 0) nt = omp_get_max_threads();
 #endif
   hitbuf* bufs = (hitbuf*)calloc((size_t)nt, sizeof(hitbuf));
   int64_t* steps = (int64_t*)calloc((size_t)nt, sizeof(int64_t));
+  /* chunk offsets: pair p owns chunks [off[p], off[p + 1]) */
+  int64_t* coff = (int64_t*)malloc((size_t)(n_pairs + 1) * sizeof(int64_t));
+  coff[0] = 0;
   for (int64_t p = 0; p < n_pairs; ++p) {
     int64_t n = pairs[p].n_photons;
     if (photon_limit >= 0 && n > photon_limit) n = photon_limit;
-#pragma omp parallel for schedule(dynamic, 1024) num_threads(nt)
-    for (int64_t ph = 0; ph < n; ++ph) {
-      int tid = 0;
+    if (n < 0) n = 0;
+    coff[p + 1] = coff[p] + (n + ORC_CHUNK - 1) / ORC_CHUNK;
+  }
+  const int64_t n_chunks = coff[n_pairs];
+  int used = 1;
+#pragma omp parallel num_threads(nt)
+  {
+    int tid = 0;
 #ifdef _OPENMP
-      tid = omp_get_thread_num();
+    tid = omp_get_thread_num();
+#pragma omp single
+    used = omp_get_num_threads();
 #endif
-      orc_hit h;
-      if (simulate_photon(t, &pairs[p], p, ph, o, &h, &steps[tid])) hb_push(&bufs[tid], &h);
+#pragma omp for schedule(dynamic, 1)
+    for (int64_t c = 0; c < n_chunks; ++c) {
+      int64_t lo = 0, hi = n_pairs - 1; /* last pair whose first chunk <= c */
+      while (lo < hi) {
+        const int64_t mid = (lo + hi + 1) / 2;
+        if (coff[mid] <= c) lo = mid; else hi = mid - 1;
+      }
+      const int64_t p = lo;
+      int64_t n = pairs[p].n_photons;
+      if (photon_limit >= 0 && n > photon_limit) n = photon_limit;
+      const int64_t b = (c - coff[p]) * ORC_CHUNK;
+      const int64_t e = b + ORC_CHUNK < n ? b + ORC_CHUNK : n;
+      for (int64_t ph = b; ph < e; ++ph) {
+        orc_hit h;
+        if (simulate_photon(t, &pairs[p], p, ph, o, &h, &steps[tid])) hb_push(&bufs[tid], &h);
+      }
     }
   }
+  free(coff);
+  if (threads_used) *threads_used = used;
   int64_t total = 0, total_steps = 0;
   for (int i = 0; i < nt; ++i) {
     total += bufs[i].n;

@@ -94,11 +94,14 @@ double orc_scattering_length(const orc_tables* t, double wl);
 /* Propagates min(n_photons, photon_limit) photons of every pair (photon_limit
  * < 0: all).  Hits are returned sorted by (pair, photon); stats is
  * [n_pairs x ORC_STATS], hist [n_pairs x hist_bins].  Returns the total number
- * of hits (which may exceed hit_cap; only hit_cap are copied). */
+ * of hits (which may exceed hit_cap; only hit_cap are copied).  The work is
+ * one flat index space of 256-photon chunks over all pairs (OpenMP, dynamic
+ * schedule), so all n_threads threads (0: OpenMP's default) work at any photon
+ * count; *threads_used (may be NULL) receives the team size that ran. */
 int64_t orc_propagate(const orc_tables* t, const orc_pair* pairs, int64_t n_pairs,
                       const orc_opts* o, int64_t photon_limit, orc_hit* hits,
                       int64_t hit_cap, double* stats, double* hist, int n_threads,
-                      int64_t* steps_out);
+                      int64_t* steps_out, int* threads_used);
 
 /* Replays one photon of a pair; returns 1 and fills *hit when it is detected. */
 int orc_simulate_one(const orc_tables* t, const orc_pair* pair, int64_t pair_idx, int64_t photon,

@@ -1,4 +1,5 @@
-"""Regenerates the package data tables from the reference checkout.
+"""Regenerates the package's PMT data tables from a PhotonProp.jl checkout
+(a maintenance script, not part of the product).
 
 pmt_acceptance.csv: the PMT quantum-efficiency curve of PhotonProp.jl
 (PMTAcc.csv, read at module load by src/detection.jl:31-33), unchanged
@@ -6,14 +7,15 @@ values, written with a header.  pmt_acceptance_5nm.csv: the same curve
 linearly interpolated at 5 nm from 300 to 700 nm (81 entries), the
 tabulation the one-pair-per-launch cone workload uses.
 
-Usage: python make_data.py /path/to/PhotonProp.jl
+Usage: python tests/golden/make_pmt_data.py /path/to/PhotonProp.jl
 """
 import os
 import sys
 
 import numpy as np
 
-HERE = os.path.dirname(os.path.abspath(__file__))
+HERE = os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
+                    "photonprop.jl_b200", "photonprop_b200", "data")
 
 
 def main(ref):
@@ -31,4 +33,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_pmt_data.py <PhotonProp.jl checkout>")
+    main(sys.argv[1])

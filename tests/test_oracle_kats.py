@@ -230,3 +230,48 @@ def test_oracle_empty_zero_photon_and_limited_pairs():
     key = lambda a: np.lexsort((a["photon"], a["pair"]))  # noqa: E731
     np.testing.assert_array_equal(hl[key(hl)]["photon"], full[key(full)]["photon"])
     np.testing.assert_array_equal(hl[key(hl)]["pos"], full[key(full)]["pos"])
+
+
+def test_oracle_flat_parallel_uses_every_thread():
+    """The oracle's work is one flat index space of (pair, 256-photon chunk)
+    items, so a batch of many pairs with fewer photons each than one chunk
+    still keeps every requested thread busy, and the result does not depend
+    on how the chunks fall on threads."""
+    T = _golden_tables()
+    rng = np.random.default_rng(3)
+    p = O.pairs_array(64)
+    p["target"] = rng.uniform(-3, 3, size=(64, 3))
+    p["radius"] = 0.21
+    p["n_photons"] = rng.integers(0, 700, size=64)
+    p["seed"] = np.arange(64) + 100
+    o = O.make_opts(mode=O.MODE_PHYSICAL, g=0.9, t_max=200.0, hist_bins=200)
+    a = O.propagate(T, p, o, n_threads=1)
+    assert O.last_threads_used == 1
+    b = O.propagate(T, p, o, n_threads=4)
+    assert O.last_threads_used == 4
+    assert a[4] == b[4] > 0 and a[3] == b[3]
+    np.testing.assert_array_equal(a[0], b[0])
+    np.testing.assert_array_equal(a[1], b[1])
+    np.testing.assert_array_equal(a[2], b[2])
+    np.testing.assert_array_equal(b[1][:, 6], p["n_photons"])
+
+
+def test_oracle_batch_generator_matches_product():
+    """oracle/batches.py draws the benchmark batch without the product
+    library (the CPU arm of the benchmark must not load it); it must be the
+    product's batch number for number."""
+    import photonprop_b200 as pp
+    from oracle import batches as ob
+    for seed, n in ((2024, 4096), (7, 33)):
+        a = pp.batches.mixed_batch(n, seed=seed)
+        b = ob.mixed_batch(n, seed=seed)
+        for f in ("pos", "t0", "dir", "track_len", "target", "radius", "n_photons", "seed", "emitter"):
+            np.testing.assert_array_equal(np.asarray(a[f], dtype=b[f].dtype), b[f], err_msg=f)
+    idx = np.array([0, 1, 2, 4095, 2**40], dtype=np.uint64)
+    for g in (0, 1, 2**63 + 5):
+        np.testing.assert_array_equal(ob.pair_seed(g, idx), [pp.propagation.pair_seed(g, int(i)) for i in idx])
+    wl, acc = ob.pmt_table()
+    np.testing.assert_array_equal(wl, pp.p_one_pmt_acc.wavelengths)
+    np.testing.assert_array_equal(acc, pp.p_one_pmt_acc.acceptance)
+    s = ob.sampled(b, 1e-3)
+    assert np.all(s["n_photons"] == np.minimum(b["n_photons"], np.maximum(1, np.ceil(b["n_photons"] * 1e-3))))
