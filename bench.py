@@ -811,6 +811,7 @@ def run_ours(args):
     MAX = dist.ReduceOp.MAX if world > 1 else None
 
     peaks = pp.measure_peaks(local)
+    sol_steps = pp.measure_step_rate(local)
     medium = pp.make_seawater(35.0, 2.0)
     spec = pp.CherenkovSpectrum((300.0, 800.0), 20, medium)
     prop = pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=local)
@@ -1020,6 +1021,12 @@ def run_ours(args):
                                 "frac": a_int / peaks["philox_blocks"]},
                      "photon_steps_per_s": steps_total / t_local,
                      "steps_per_photon": steps_total / max(sum(photons_local), 1),
+                     "step_speed_of_light": {
+                         "steps_per_s": sol_steps,
+                         "what": "bare physical step on every SM (Philox block, ray-sphere, move, turn; no emission, "
+                                 "refill, hits or loop bookkeeping), pp_measure_step_rate",
+                         "mufu_frac_ceiling": roofline.MUFU_PER_STEP * sol_steps / peaks["mufu_ops"],
+                         "batched_steps_frac": steps_total / t_local / sol_steps},
                      "hbm": {"achieved_gbs": hits_local * 64 / t_local / 1e9, "peak_gbs": measured_hbm_gbs(),
                              "what": "hit write-back", "peak_source": "MEASURED_PEAKS.json hbm_gbs"}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n_pairs * 80,

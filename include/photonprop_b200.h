@@ -545,6 +545,14 @@ PP_API pp_status pp_device_eval(pp_ctx* ctx, int32_t op, const double* in, doubl
 PP_API pp_status pp_measure_peaks(int device, double* fp32_ops_per_s, double* mufu_ops_per_s,
                            double* philox_blocks_per_s);
 
+/* Speed of light of the physical photon step on this device: photon steps
+ * per second when every lane of every SM steps its own photon (one
+ * Philox4x32-10 block, ray-sphere test, move, Henyey-Greenstein turn) with no
+ * emission, refill, hit record or loop bookkeeping, at the batched kernel's
+ * occupancy.  No reference counterpart: the ceiling the batched kernel's
+ * step rate is reported against. */
+PP_API pp_status pp_measure_step_rate(int device, double* steps_per_s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1055,6 +1055,20 @@ pp_status pp_measure_peaks(int device, double* fp32, double* mufu, double* iops)
   return e ? PP_ERR_CUDA : PP_OK;
 }
 
+pp_status pp_measure_step_rate(int device, double* steps_per_s) {
+  if (!steps_per_s) return PP_ERR_ARG;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return PP_ERR_ARG;
+  }
+  DeviceGuard guard(device);
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, device);
+  cudaError_t e = pp::run_step_rate(prop.multiProcessorCount, steps_per_s);
+  return e ? PP_ERR_CUDA : PP_OK;
+}
+
 // Autotuner: times the batched kernel over a grid of launch shapes on the
 // given pairs and keeps the fastest per mode.  The cache file holds one line
 // per (device name, mode): "name|mode|block|blocks_per_sm|chunk|photons_per_s".

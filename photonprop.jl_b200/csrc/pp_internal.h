@@ -66,6 +66,7 @@ cudaError_t launch_eval(int op, const double* in, double* out, int64_t n, const 
 int batched_max_blocks_per_sm(int mode, int block, bool cascade);
 int plain_max_blocks_per_sm(int mode, int block);
 cudaError_t run_peaks(int sm_count, double* fp32, double* mufu, double* iops);
+cudaError_t run_step_rate(int sm_count, double* steps_per_s);
 
 // batched launch with caller-owned scratch, direct launches (pp_capi.cu)
 pp_status propagate_with_scratch(pp_ctx* c, const pp_pair* d_pairs, int64_t n_pairs, const pp_run_opts* opts,

@@ -533,6 +533,41 @@ __global__ void peak_philox_kernel(unsigned* out, int iters) {
   if (acc == 12345u) out[0] = acc;
 }
 
+// Speed of light of the physical step: every lane steps its own photon
+// through step_event (one Philox4x32-10 block, the ray-sphere test, the move
+// and the Henyey-Greenstein turn) with no emission, refill, hit record or
+// loop bookkeeping, at the batched kernel's occupancy (256 threads, 4 CTAs
+// per SM, at most 64 registers).  Its step rate bounds what the batched
+// kernel can reach on this GPU under instruction-issue limits.  The photons
+// start 100 m from a 0.21 m sphere with an unbounded path, so they keep
+// moving; the results are kept live through a never-true store.
+__global__ void __launch_bounds__(256, 4) peak_step_kernel(const RunParams R, int iters,
+                                                           unsigned long long* __restrict__ out) {
+  PairCtx c;
+  c.r = 0.21f;
+  c.seed_lo = 0x9E3779B9u * (blockIdx.x + 1u);
+  c.seed_hi = 0x2545F491u;
+  c.index = 0;
+  Photon s;
+  s.id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  s.px = 100.f + (float)(threadIdx.x & 31u);
+  s.py = 50.f;
+  s.pz = -30.f;
+  s.dx = 0.6f;
+  s.dy = 0.f;
+  s.dz = 0.8f;
+  s.path = 1e30f;
+  s.neg_ln2_len = -kLn2 * 30.f;
+  s.ctr3 = ctr_word(s.id, 1u);
+  unsigned live = 0;
+  for (int i = 0; i < iters; ++i) {
+    bool hit = false;
+    live += step_event<kPhysical>(R, c, s, hit) ? 1u : 0u;
+  }
+  if (s.px == 1.2345f && s.dz == 0.5f && live == 7u) out[1] = 1ull;
+  if ((threadIdx.x & 31u) == 0) atomicAdd(out, 32ull * (unsigned long long)iters);
+}
+
 }  // namespace ppd
 
 // ---------------------------------------------------------------------------
@@ -767,6 +802,38 @@ cudaError_t run_peaks(int sm_count, double* fp32, double* mufu, double* iops) {
   e = cudaGetLastError();
   cudaEventDestroy(a);
   cudaEventDestroy(b);
+  cudaFree(dout);
+  return e;
+}
+
+cudaError_t run_step_rate(int sm_count, double* steps_per_s) {
+  unsigned long long* dout = nullptr;
+  cudaError_t e = cudaMalloc(&dout, 16);
+  if (e != cudaSuccess) return e;
+  cudaMemset(dout, 0, 16);
+  LaunchArgs a{};
+  a.opts.mode = PP_MODE_PHYSICAL;
+  a.opts.max_steps = 1000;
+  a.opts.g = 0.95f;
+  a.opts.t_max = 1000.f;
+  ppd::RunParams R = to_params(a);
+  R.ctr_limit = 0xFFFFFFFFu;
+  cudaEvent_t t0, t1;
+  cudaEventCreate(&t0);
+  cudaEventCreate(&t1);
+  const int grid = sm_count * 4, block = 256, iters = 20000;
+  ppd::peak_step_kernel<<<grid, block>>>(R, 500, dout);  // warm-up
+  cudaEventRecord(t0);
+  ppd::peak_step_kernel<<<grid, block>>>(R, iters, dout);
+  cudaEventRecord(t1);
+  cudaEventSynchronize(t1);
+  count_launches(2);
+  float ms = 0.f;
+  cudaEventElapsedTime(&ms, t0, t1);
+  *steps_per_s = (double)grid * block * iters / (ms * 1e-3);
+  e = cudaGetLastError();
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
   cudaFree(dout);
   return e;
 }

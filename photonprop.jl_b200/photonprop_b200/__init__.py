@@ -41,3 +41,14 @@ def measure_peaks(device=0):
     f, m, i = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
     _lib.check(L.pp_measure_peaks(device, ctypes.byref(f), ctypes.byref(m), ctypes.byref(i)))
     return {"fp32_ops": f.value, "mufu_ops": m.value, "philox_blocks": i.value}
+
+
+def measure_step_rate(device=0):
+    """Photon steps per second of the bare physical step on every SM (one
+    Philox block, ray-sphere test, move, turn; no emission, refill, hit
+    record or loop bookkeeping): the speed of light of the step loop."""
+    import ctypes
+    L = _lib.load()
+    r = ctypes.c_double()
+    _lib.check(L.pp_measure_step_rate(device, ctypes.byref(r)))
+    return r.value

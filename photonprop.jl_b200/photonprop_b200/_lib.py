@@ -169,6 +169,7 @@ _SIGS = [
     ("pp_device_eval", ctypes.c_int, [_VP, _I32, _VP, _VP, _I64]),
     ("pp_measure_peaks", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_D), ctypes.POINTER(_D),
                                         ctypes.POINTER(_D)]),
+    ("pp_measure_step_rate", ctypes.c_int, [ctypes.c_int, ctypes.POINTER(_D)]),
 ]
 
 EXPORTED = [s[0] for s in _SIGS]

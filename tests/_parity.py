@@ -72,3 +72,80 @@ def chi2_two_sample(a, b, min_count=10):
     chi2 = float(np.sum((ka * ra - kb * rb) ** 2 / (ra + rb)))
     dof = len(ra) - 1
     return chi2, dof, float(st.chi2.sf(chi2, dof))
+
+
+def check_matched(g, o, n_gpu_only, n_orc_only, label, flip_frac=0.01, flip_abs=3):
+    """Per-photon tolerances of matched hits (GPU FP32 against the FP64 oracle
+    on the same Philox numbers):  |d pos| <= 2e-3 m + 2e-5 path,
+    |d t| <= 1e-2 ns + 1e-5 t, |d w| <= 1e-3 w + 1e-8, |d lambda| / lambda <= 1e-5;
+    photons detected on one side only (sphere-rim flips) <= flip_frac of the
+    hits + flip_abs."""
+    err = per_photon_errors(g, o)
+    s = summary(err)
+    print(label, "matched", len(g), "gpu-only", n_gpu_only, "oracle-only", n_orc_only, s)
+    n = max(len(g), 1)
+    assert n_gpu_only + n_orc_only <= flip_frac * n + flip_abs, (label, n_gpu_only, n_orc_only, len(g))
+    path = o["dist"]
+    assert np.all(err["pos"] <= 2e-3 + 2e-5 * path), (label, s["pos"])
+    assert np.all(err["time"] <= 1e-2 + 1e-5 * o["time"]), (label, s["time"])
+    # relative 1e-3, plus an absolute floor where the PMT acceptance tends to zero
+    assert np.all(np.abs(g["weight"] - o["weight"]) <= 1e-3 * o["weight"] + 1e-8), (label, s["weight"])
+    assert np.all(err["wavelength"] <= 1e-5), (label, s["wavelength"])
+    return s
+
+
+def _split(gpu_hits, orc_hits):
+    gk = {(int(h["pair"]), int(h["photon"])): i for i, h in enumerate(gpu_hits)}
+    ok = {(int(h["pair"]), int(h["photon"])): i for i, h in enumerate(orc_hits)}
+    both = sorted(set(gk) & set(ok))
+    g_only = np.array(sorted(gk[k] for k in set(gk) - set(ok)), dtype=np.int64)
+    o_only = np.array(sorted(ok[k] for k in set(ok) - set(gk)), dtype=np.int64)
+    gi = np.array([gk[k] for k in both], dtype=np.int64)
+    oi = np.array([ok[k] for k in both], dtype=np.int64)
+    return gi, oi, g_only, o_only
+
+
+def check_pair_statistics_and_histograms(gpu_res, orc_hits, orc_stats, orc_hist, n_pairs, t0, width, bins,
+                                         label, edge_ns=1e-2):
+    """Reconciles the kernel's FP64 per-pair sums and arrival-time histograms
+    with the oracle's, bin by bin.  The oracle's table, with its one-sided
+    photons (rim flips) replaced by the GPU's and any matched photon whose
+    time lies within edge_ns of a bin edge moved to the GPU's bin, must equal
+    the GPU's: hit counts exactly, weights to 2e-3 relative."""
+    gh = gpu_res.hits
+    gi, oi, g_only, o_only = _split(gh, orc_hits)
+    g_t = gh["time"].astype(np.float64)
+    g_w = gh["weight"].astype(np.float64)
+    g_p = gh["pair"].astype(np.int64)
+    o_t, o_w, o_p = orc_hits["time"], orc_hits["weight"], orc_hits["pair"].astype(np.int64)
+
+    def bin_of(t):
+        return np.floor((t - t0) / width)
+
+    exp_hist = orc_hist.copy()
+    exp_cnt = orc_stats[:, 0].copy()
+    exp_w = orc_stats[:, 1].copy()
+
+    def add(p, t, w, sign):
+        b = bin_of(t)
+        inside = (b >= 0) & (b < bins)
+        np.add.at(exp_hist, (p[inside], b[inside].astype(np.int64)), sign * w[inside])
+
+    add(o_p[o_only], o_t[o_only], o_w[o_only], -1.0)
+    add(g_p[g_only], g_t[g_only], g_w[g_only], +1.0)
+    np.add.at(exp_cnt, o_p[o_only], -1.0)
+    np.add.at(exp_cnt, g_p[g_only], +1.0)
+    np.add.at(exp_w, o_p[o_only], -o_w[o_only])
+    np.add.at(exp_w, g_p[g_only], +g_w[g_only])
+    moved = bin_of(g_t[gi]) != bin_of(o_t[oi])
+    if np.any(moved):
+        tt = o_t[oi][moved]
+        edge = t0 + width * np.round((tt - t0) / width)
+        assert np.all(np.abs(tt - edge) <= edge_ns), (label, "bin differs away from an edge")
+        add(o_p[oi][moved], o_t[oi][moved], o_w[oi][moved], -1.0)
+        add(g_p[gi][moved], g_t[gi][moved], g_w[gi][moved], +1.0)
+    s = gpu_res.stats
+    np.testing.assert_array_equal(s[:, 0], exp_cnt, err_msg=label)
+    np.testing.assert_allclose(s[:, 1], exp_w, rtol=2e-3, atol=1e-12, err_msg=label)
+    np.testing.assert_allclose(gpu_res.hist[:, :bins], exp_hist, rtol=2e-3, atol=1e-12, err_msg=label)
+    return int(np.count_nonzero(moved))
