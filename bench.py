@@ -54,9 +54,13 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-tune", action="store_true")
-    ap.add_argument("--serving-seconds", type=float, default=10.0,
-                    help="length of the serving sample in the default run (0 = skip)")
+    ap.add_argument("--serving-seconds", type=float, default=60.0,
+                    help="length of the serving sample in the default run (0 = skip; one GPU only)")
     ap.add_argument("--serving-rate", type=float, default=200.0, help="request arrival rate, Hz")
+    ap.add_argument("--overload-rate", type=float, default=2000.0,
+                    help="arrival rate of the second, overload serving sample, Hz")
+    ap.add_argument("--overload-seconds", type=float, default=10.0,
+                    help="length of the overload serving sample (0 = skip)")
     ap.add_argument("--workload", choices=["batch", "serving", "surrogate", "surrogate-infer", "cone-grid", "point",
                                            "fits", "event", "llh"], default="batch")
     ap.add_argument("--fit-photons", type=int, default=100_000_000, help="fits workload: photons per distance")
@@ -980,9 +984,15 @@ def run_ours(args):
 
     surrogate_inf = surrogate_inference_rate(local)
 
+    # serving: the configured stream (Poisson 200 req/s) and an overload sample where the one-launch-
+    # per-request loop saturates; one GPU only (the scaling runs measure the batch)
     serve = None
-    if args.serving_seconds > 0:
-        serve = run_serving(prop, args.serving_seconds, seed=args.seed + rank)
+    if args.serving_seconds > 0 and world == 1:
+        serve = {"configured": run_serving(prop, args.serving_seconds, seed=args.seed + rank,
+                                           rate_hz=args.serving_rate)}
+        if args.overload_seconds > 0:
+            serve["overload"] = run_serving(prop, args.overload_seconds, seed=args.seed + 17 + rank,
+                                            rate_hz=args.overload_rate)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -242,9 +242,11 @@ PP_API pp_status pp_propagate_device(pp_ctx* ctx, const pp_pair* d_pairs, int64_
  * nothing, launches directly (no graph) and otherwise behaves like
  * pp_propagate_device.  Limits and rules:
  *  - n_pairs above PP_NOALLOC_MAX_PAIRS is rejected with PP_ERR_ARG;
- *  - the first call on a device looks up the array's device address (once per
- *    device, with that device current); make that first call before any stream
- *    capture;
+ *  - every call looks up the array's device address with the context's
+ *    device current; the first call on a device is the set-up (it may load the
+ *    library's device code there), so make that first call before any stream
+ *    capture; later lookups allocate nothing, and after a device reset the
+ *    call finds the new context's array;
  *  - all calls share the array and it keeps the last call's contents (each
  *    call resets what must start at zero), so calls that overlap on the GPU
  *    race: issue them on one stream or otherwise serialise them. */

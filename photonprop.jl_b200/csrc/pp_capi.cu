@@ -1218,27 +1218,22 @@ cudaError_t ctx_llh_scratch(pp_ctx* c, size_t bytes, void** out) {
 // the name g_noalloc_scratch is only a host-side stand-in for the symbol, not
 // a device address: a kernel given it would fault or, where the GPU can reach
 // host memory, silently use the wrong memory.  The device address is looked
-// up once per device with cudaGetSymbolAddress (with that device current) and
-// cached.
+// up with cudaGetSymbolAddress with the context's device current.  The first
+// lookup on a device is the set-up (it may load the library's device code
+// there); later lookups allocate nothing.  The lookup is repeated on every
+// call rather than cached, so that after a device reset (cudaDeviceReset,
+// CUDA.jl's device_reset!) the call uses the array of the new context
+// instead of the old one's address.
 namespace {
 constexpr int kNoallocQueueWords = 32;
 static __device__ __align__(256) unsigned long long g_noalloc_scratch[kNoallocQueueWords + PP_NOALLOC_MAX_PAIRS + 1];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_noalloc_mu;
-unsigned long long* g_noalloc_ptr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device (set-up on first use).
-cudaError_t noalloc_scratch(int device, unsigned long long** out) {
-  std::lock_guard<std::mutex> lk(g_noalloc_mu);
-  if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-  if (!g_noalloc_ptr[device]) {
-    void* p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess) return e;
-    g_noalloc_ptr[device] = static_cast<unsigned long long*>(p);
-  }
-  *out = g_noalloc_ptr[device];
+// Device address of the scratch array on the current device.
+cudaError_t noalloc_scratch(unsigned long long** out) {
+  void* p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return e;
+  *out = static_cast<unsigned long long*>(p);
   return cudaSuccess;
 }
 }  // namespace
@@ -1247,6 +1242,7 @@ extern "C" pp_status pp_propagate_device_noalloc(pp_ctx* c, const pp_pair* d_pai
                                                  const pp_run_opts* opts, pp_hit* d_hits, int64_t cap,
                                                  uint64_t* d_counters, double* d_stats, double* d_hist,
                                                  void* stream) {
+  pp::Range range_("pp_propagate_device_noalloc");
   if (!c) return PP_ERR_ARG;
   std::lock_guard<std::mutex> lk(c->mu);
   pp_status st = validate_opts(c, opts);
@@ -1263,7 +1259,7 @@ extern "C" pp_status pp_propagate_device_noalloc(pp_ctx* c, const pp_pair* d_pai
                    "pp_propagate_device_noalloc: pairs/hits need 16-byte, counters/stats/hist 8-byte alignment");
   DeviceGuard guard(c->device);
   unsigned long long* scratch = nullptr;
-  cudaError_t e = noalloc_scratch(c->device, &scratch);
+  cudaError_t e = noalloc_scratch(&scratch);
   if (e) return c->cuda_fail(e, "pp_propagate_device_noalloc: cudaGetSymbolAddress");
   int grid, block;
   uint32_t chunk;

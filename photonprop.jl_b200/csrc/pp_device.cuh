@@ -422,12 +422,17 @@ __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& 
   s.ctr3 = ctr_word(s.id, 1u);
 }
 
-// Step k (block k + 1) of src/photon_prop_cuda.jl:320-376: step length,
-// ray-sphere test, move, Henyey-Greenstein turn.  Returns false when the
-// photon ends; *hit is set when it ends on the sphere (position and path
-// length then at the hit).
+// Step k (block k + 1) of src/photon_prop_cuda.jl:320-376, first half: step
+// length, ray-sphere test and move.  Returns false when the photon ends;
+// *hit is set when it ends on the sphere (position and path length then at
+// the hit, direction the arrival direction), *turn when the step's
+// Henyey-Greenstein turn applies (step_turn with the returned u1, u2).  The
+// turn is split off so that a kernel can record the step's hits first and
+// then turn with predicated writes instead of selects between the old and the
+// new direction.
 template <int MODE>
-__device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c, Photon& s, bool& hit) {
+__device__ __forceinline__ bool step_move(const RunParams& R, const PairCtx& c, Photon& s, bool& hit, bool& turn,
+                                          float& u1, float& u2) {
   const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, s.ctr3);
   const float step = lg2(d.u0) * s.neg_ln2_len;
   const float ex = s.px, ey = s.py, ez = s.pz;  // photon - sphere centre
@@ -439,16 +444,18 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
   const float q = fmaf(qz, qz, fmaf(qy, qy, qx * qx));
   const float b = fmaf(c.r, c.r, -q);
   const float pp = fmaf(a, a, q);  // |e|^2
-  // branch-free decisions: the line meets the sphere (b >= 0) at dd ahead
-  // (b < 0 makes dd NaN, which no decision reads: line is false)
+  // the line meets the sphere at dd ahead (b < 0: the approximate square root
+  // of a negative number is NaN, so dd is NaN and every comparison below is
+  // false: no intersection)
   const float dd = -a - sqrt_a(b);
-  const bool line = b >= 0.f;
-  const bool geo = line && dd > 0.f && dd < step;  // reaches the sphere within this step
+  const bool geo = dd > 0.f && dd < step;  // reaches the sphere within this step
   bool alive, move;
+  float len;
   if (MODE == kCompat) {
     hit = geo;
-    move = !line;  // the line meets the sphere outside this step: no move (reference)
+    move = !(b >= 0.f);  // the line meets the sphere outside this step: no move (reference)
     alive = !geo;
+    len = hit ? dd : (move ? step : 0.f);
   } else {
     hit = geo && dd <= s.path;  // arrives inside the time window
     // A photon farther from the sphere than the path it has left before t_max
@@ -458,20 +465,34 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
     const float reach = fmaf(s.path, 1.0001f, c.r + 0.05f);
     move = !geo && step <= s.path && pp <= reach * reach;
     alive = move;
+    len = geo ? dd : step;  // a photon that ends without a hit keeps no state
   }
-  const float len = hit ? dd : (move ? step : 0.f);
   s.px = fmaf(len, s.dx, s.px);
   s.py = fmaf(len, s.dy, s.py);
   s.pz = fmaf(len, s.dz, s.pz);
   s.path += (MODE == kPhysical) ? -len : len;
-  const float cpol = hg_costheta(R.hg, d.u1);
-  float rx, ry, rz;
-  polar_direction<false>(s.dx, s.dy, s.dz, cpol, sin_from_cos(cpol), d.u2, rx, ry, rz);
-  s.dx = move ? rx : s.dx;
-  s.dy = move ? ry : s.dy;
-  s.dz = move ? rz : s.dz;
   s.ctr3 += 1u << 8;
+  turn = move;
+  u1 = d.u1;
+  u2 = d.u2;
   return alive && s.ctr3 < R.ctr_limit;  // at most max_steps steps
+}
+
+// Second half of the step: the Henyey-Greenstein turn
+// (src/photon_prop_cuda.jl:223-241 via update_direction).
+__device__ __forceinline__ void step_turn(const RunParams& R, Photon& s, float u1, float u2) {
+  const float cpol = hg_costheta(R.hg, u1);
+  polar_direction<false>(s.dx, s.dy, s.dz, cpol, sin_from_cos(cpol), u2, s.dx, s.dy, s.dz);
+}
+
+// The whole step (move, then the turn if it applies).
+template <int MODE>
+__device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c, Photon& s, bool& hit) {
+  bool turn;
+  float u1, u2;
+  const bool alive = step_move<MODE>(R, c, s, hit, turn, u1, u2);
+  if (turn) step_turn(R, s, u1, u2);
+  return alive;
 }
 
 // Emission (block 0) or step event of one photon.

@@ -195,6 +195,7 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
     if (!alive) {
       const unsigned rank = __popc(need & lt_mask);
       if (rank < r_count) {
+        steps += (s.ctr3 >> 8) - 1u;  // the ended photon's steps (block = steps + 1)
         const float4* src = reinterpret_cast<const float4*>(ring + ((r_head + rank) & (kStage - 1)));
         const float4 a = src[0], b = src[1], d = src[2], e = src[3];
         s.px = a.x;
@@ -219,12 +220,12 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
     r_count -= took;
     __syncwarp();
     if (need == kFull && took == 0u) break;  // every lane was idle and none took a photon
-    bool hit = false;
-    if (alive) {
-      ++steps;
-      alive = step_event<MODE>(R, c, s, hit);
-    }
+    bool hit = false, turn = false;
+    float u1 = 0.f, u2 = 0.f;
+    if (alive) alive = step_move<MODE>(R, c, s, hit, turn, u1, u2);
     if (MODE == kCompat) {
+      // a hit lane does not turn, so the turn can precede the hit staging
+      if (turn) step_turn(R, s, u1, u2);
       const unsigned hm = __ballot_sync(kFull, hit);
       if (hm) {
         const unsigned nh = __popc(hm);
@@ -258,7 +259,11 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         record_hit_cached(R, ws, c, s, h);
       }
     }
+    // physical mode turns after the hit record (which needs the arrival
+    // direction): predicated writes of the new direction, no selects
+    if (MODE == kPhysical && turn) step_turn(R, s, u1, u2);
   }
+  steps += (s.ctr3 >> 8) - 1u;  // the last photon's steps
   __syncwarp();
   if (MODE == kCompat && h_count > 0u) record_staged(h_count);
   if (lane == 0) flush_warp_stats(R.stats, ws);

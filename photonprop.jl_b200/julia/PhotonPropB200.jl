@@ -13,6 +13,7 @@ module PhotonPropB200
 
 export PPMediumDesc, PPSpectrumDesc, PPPmtDesc, PPPair, PPRunOpts, PPHit
 export Context, propagate_pairs, propagate_distance, default_opts, make_photon_fits, get_dir_reweight
+export propagate_device!, propagate_device_noalloc!
 
 const libpp = get(ENV, "PHOTONPROP_B200_LIB",
                   joinpath(@__DIR__, "..", "libphotonprop_b200.so"))
@@ -155,6 +156,46 @@ function propagate_pairs(ctx::Context, pairs::Vector{PPPair}, opts::PPRunOpts; h
                ctx.ptr, pairs, n, opts, hits, hit_capacity, nh, stats, opts.hist_bins > 0 ? hist : C_NULL)
     st == PP_ERR_OVERFLOW || check(st, ctx.ptr)
     (hits[1:min(nh[], hit_capacity)], nh[], stats, hist)
+end
+
+"""
+    propagate_device!(ctx, d_pairs, n_pairs, opts, d_hits, hit_capacity, d_counters, d_stats, d_hist, stream)
+
+`pp_propagate_device` on device buffers (raw device addresses, e.g.
+`UInt(pointer(A))` of CuArrays: `d_pairs` n_pairs `PPPair`s, `d_hits`
+hit_capacity `PPHit`s, `d_counters` 4 `UInt64`, `d_stats` PP_STATS x n_pairs
+and `d_hist` hist_bins x n_pairs `Float64`), asynchronous on the `CUstream`
+`stream` (CUDA.jl: `CUDA.stream().handle`; `C_NULL` for the default stream).
+"""
+function propagate_device!(ctx::Context, d_pairs, n_pairs::Integer, opts::PPRunOpts, d_hits, hit_capacity::Integer,
+                           d_counters, d_stats, d_hist, stream=C_NULL)
+    check(ccall((:pp_propagate_device, libpp), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ref{PPRunOpts}, Ptr{Cvoid}, Int64, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid},
+                 Ptr{Cvoid}),
+                ctx.ptr, Ptr{Cvoid}(UInt(d_pairs)), n_pairs, opts, Ptr{Cvoid}(UInt(d_hits)), hit_capacity,
+                Ptr{Cvoid}(UInt(d_counters)), Ptr{Cvoid}(UInt(d_stats)), Ptr{Cvoid}(UInt(d_hist)),
+                Ptr{Cvoid}(UInt(stream))), ctx.ptr)
+    nothing
+end
+
+"""
+    propagate_device_noalloc!(ctx, d_pairs, n_pairs, opts, d_hits, hit_capacity, d_counters, d_stats, d_hist, stream)
+
+The same call for code that keeps all device memory in CUDA.jl's pool
+(`pp_propagate_device_noalloc`): the library allocates nothing, its work-queue
+scratch being a fixed ~512 KiB device array.  At most 65536 pairs per call;
+make the first call on a device before any stream capture; calls that
+overlap on the GPU race on the shared scratch, so issue them on one stream.
+"""
+function propagate_device_noalloc!(ctx::Context, d_pairs, n_pairs::Integer, opts::PPRunOpts, d_hits,
+                                   hit_capacity::Integer, d_counters, d_stats, d_hist, stream=C_NULL)
+    check(ccall((:pp_propagate_device_noalloc, libpp), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Int64, Ref{PPRunOpts}, Ptr{Cvoid}, Int64, Ptr{Cvoid}, Ptr{Cvoid}, Ptr{Cvoid},
+                 Ptr{Cvoid}),
+                ctx.ptr, Ptr{Cvoid}(UInt(d_pairs)), n_pairs, opts, Ptr{Cvoid}(UInt(d_hits)), hit_capacity,
+                Ptr{Cvoid}(UInt(d_counters)), Ptr{Cvoid}(UInt(d_stats)), Ptr{Cvoid}(UInt(d_hist)),
+                Ptr{Cvoid}(UInt(stream))), ctx.ptr)
+    nothing
 end
 
 const C_VAC = 0.299792458  # m/ns
