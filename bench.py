@@ -784,6 +784,53 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def plain_by_pair_size(prop, ro, b, d_batch, d_pair_views, h_pairs, d_hits, cap, d_cnt, d_st1, d_hi1, d_stats,
+                       d_hist, s, flush):
+    """Where the one-pair-per-launch path loses against the batched kernel:
+    per-pair device time of the plain path (its memsets, counter reset,
+    kernel and finalisation, launched back to back as in the plain pass) and
+    the batched kernel on each photon-count decade of the same batch alone,
+    photons/s per decade, plus the plain path's fixed cost per pair (the
+    median time of the pairs below 2e4 photons)."""
+    import torch
+    n = np.asarray(b["n_photons"], dtype=np.int64)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(len(b))]
+    with torch.cuda.stream(s):
+        flush.fill_(3)
+    for i in range(len(b)):
+        ev[i][0].record(s)
+        prop.propagate_plain_device(d_pair_views[i], h_pairs[i], i, ro, d_hits, cap, d_cnt, d_st1, d_hi1, stream=s)
+        ev[i][1].record(s)
+    s.synchronize()
+    t = np.array([a.elapsed_time(e) / 1e3 for a, e in ev])
+    out = {"what": "plain: per-pair device time (memsets, reset, kernel, finalisation) summed per decade; batched: "
+                   "the decade's pairs as one batched launch",
+           "plain_fixed_cost_us_per_pair": float(np.median(t[n < 20000]) * 1e6) if np.any(n < 20000) else None,
+           "decades": []}
+    for lo, hi in ((1e4, 1e5), (1e5, 1e6), (1e6, 1e7 + 1)):
+        sel = np.nonzero((n >= lo) & (n < hi))[0]
+        if len(sel) == 0:
+            continue
+        ph = float(n[sel].sum())
+        sub = np.ascontiguousarray(b[sel])
+        d_sub = torch.from_numpy(sub.view(np.uint8).copy()).to(d_batch.device)
+        for _ in range(2):
+            prop.propagate_device(d_sub, len(sel), ro, d_hits, cap, d_cnt, d_stats, d_hist, stream=s)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(s):
+            flush.fill_(5)
+        e0.record(s)
+        prop.propagate_device(d_sub, len(sel), ro, d_hits, cap, d_cnt, d_stats, d_hist, stream=s)
+        e1.record(s)
+        s.synchronize()
+        tb = e0.elapsed_time(e1) / 1e3
+        tp = float(t[sel].sum())
+        out["decades"].append({"photons": [lo, min(hi, 1e7)], "pairs": int(len(sel)), "photon_share": ph / n.sum(),
+                               "plain_photons_per_s": ph / tp, "batched_photons_per_s": ph / tb,
+                               "batched_over_plain": tp / tb, "plain_time_share": tp / t.sum()})
+    return out
+
+
 # ---------------------------------------------------------------------------
 def run_ours(args):
     import torch
@@ -890,10 +937,14 @@ def run_ours(args):
     iso = [int(batches[W + k]["n_photons"][batches[W + k]["emitter"] == 0].sum()) for k in range(K)]
     cone = [photons_local[k] - iso[k] for k in range(K)]
     steps_total = int(cnt[:, 1].sum())
-    mufu, fp32, iops = roofline.op_counts(steps_total, sum(iso), sum(cone))
+    mufu, fp32, iops = roofline.op_counts(steps_total, sum(iso), sum(cone), algorithmic=True)
+    mufu_i, fp32_i, _ = roofline.op_counts(steps_total, sum(iso), sum(cone), algorithmic=False)
     a_mufu, a_fp32, a_int = mufu / t_local, fp32 / t_local, iops / t_local
     f_mufu, f_fp32 = a_mufu / peaks["mufu_ops"], a_fp32 / peaks["fp32_ops"]
     hits_local = int(cnt[:, 0].sum())
+    # algorithmic HBM bytes over the K steps: pairs in, hits out, histograms and statistics zeroed and written,
+    # chunk offsets written and read
+    alg_bytes = K * (n_pairs * 80 + 2 * n_pairs * (bins + 8) * 8 + 2 * (n_pairs + 1) * 8) + hits_local * 64
 
     # plain: one launch per pair on the same batch, kernels only (no host sync
     # between pairs) and through the host-buffer API (sync + copy-back per pair)
@@ -931,6 +982,8 @@ def run_ours(args):
                  "launches_per_pass": 3 * n_pairs}
         plain["batched_over_plain_kernel"] = value / plain["kernel_photons_per_s"]
         plain["batched_over_plain_host_api"] = value / plain["host_api_photons_per_s"]
+        plain["by_pair_size"] = plain_by_pair_size(prop, ro, b, d_pairs[W], d_pair_views, h_pairs, d_hits, cap,
+                                                   d_cnt, d_st1, d_hi1, d_stats, d_hist, s, flush)
         # the reference's own launch shape: cuda_propagate_photons! as propagate_distance launches
         # it (16 blocks x 1024 threads, per-block hit stacks), one pair per launch, on the first
         # 256 pairs of the same batch
@@ -1026,6 +1079,12 @@ def run_ours(args):
                          roofline.NCU_ISSUE_ACTIVE, roofline.NCU_PIPES["alu"], roofline.NCU_PIPES["fma"],
                          roofline.NCU_PIPES["xu"]),
                      "peak_source": "measured live: ex2.approx dependent chains over every SM (pp_measure_peaks)",
+                     "counts": "achieved = algorithmic MUFU operations (the reference's arithmetic: 7 per photon "
+                               "step, 10 per isotropic / 14 per cone photon start) per second; 'issued' = this "
+                               "kernel's own count of the same work (6 per step)",
+                     "issued": {"mufu_achieved": mufu_i / t_local / 1e9,
+                                "mufu_frac": mufu_i / t_local / peaks["mufu_ops"],
+                                "fp32_frac": fp32_i / t_local / peaks["fp32_ops"]},
                      "fp32": {"achieved": a_fp32 / 1e9, "peak": peaks["fp32_ops"] / 1e9, "frac": f_fp32},
                      "philox": {"achieved_blocks_per_s": a_int, "peak_blocks_per_s": peaks["philox_blocks"],
                                 "frac": a_int / peaks["philox_blocks"]},
@@ -1035,10 +1094,18 @@ def run_ours(args):
                          "steps_per_s": sol_steps,
                          "what": "bare physical step on every SM (Philox block, ray-sphere, move, turn; no emission, "
                                  "refill, hits or loop bookkeeping), pp_measure_step_rate",
-                         "mufu_frac_ceiling": roofline.MUFU_PER_STEP * sol_steps / peaks["mufu_ops"],
-                         "batched_steps_frac": steps_total / t_local / sol_steps},
-                     "hbm": {"achieved_gbs": hits_local * 64 / t_local / 1e9, "peak_gbs": measured_hbm_gbs(),
-                             "what": "hit write-back", "peak_source": "MEASURED_PEAKS.json hbm_gbs"}},
+                         "mufu_frac_ceiling": roofline.MUFU_PER_STEP_ALG * sol_steps / peaks["mufu_ops"],
+                         "mufu_frac_ceiling_issued": roofline.MUFU_PER_STEP * sol_steps / peaks["mufu_ops"],
+                         "batched_steps_frac": steps_total / t_local / sol_steps,
+                         "frac_of_ceiling": f_mufu / (roofline.MUFU_PER_STEP_ALG * sol_steps / peaks["mufu_ops"])},
+                     "hbm": {"achieved_gbs": alg_bytes / t_local / 1e9, "peak_gbs": measured_hbm_gbs(),
+                             "frac": alg_bytes / t_local / 1e9 / measured_hbm_gbs(),
+                             "algorithmic_bytes_per_step": alg_bytes / K,
+                             "what": "algorithmic HBM bytes of a step: pair records read (80 B each), hit records "
+                                     "written (64 B each), the FP64 histograms and statistics written (zeroed, then "
+                                     "the accumulated table), the work-queue offsets written and read",
+                             "peak_source": "MEASURED_PEAKS.json hbm_gbs (else 6650 GB/s, an earlier measurement "
+                                            "on this pool)"}},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": n_pairs * 80,
                 "d2h_bytes_per_step": int(d2h / K)},
         "plain": plain,

@@ -204,46 +204,100 @@ __device__ __forceinline__ void load_tile(__nv_bfloat16* dst, const __nv_bfloat1
 // Inference: persistent over 128-row tiles.  x [n][4] raw features; out
 // [5][n] (structure of arrays): raw = the de-standardised network outputs
 // (ln(mu/N), logit w, ln a1, ln a2, ln theta); physical = (mu, w, a1, a2, theta).
-__global__ void __launch_bounds__(THREADS, 1) infer_kernel(DevParams P, const float* __restrict__ x,
-                                                          float* __restrict__ out, int64_t n, int physical) {
+//
+// One CTA per SM with kGroups independent groups of 128 threads (four
+// warps, one query row per thread).  The groups share the BF16 weight tiles
+// of layers 2 and 3 in shared memory; each owns an activation tile, an
+// mbarrier and 128 of the CTA's TMEM columns, and walks its own sequence of
+// row tiles with group-local named barriers.  While one group's MMAs run on
+// the tensor cores the others run their bias/GELU epilogues on the FP32 and
+// MUFU pipes, and sixteen warps per SM keep those pipes busy.
+constexpr int kGroups = 4, INFER_THREADS = kGroups * THREADS;
+
+__device__ __forceinline__ void group_sync(int g) {
+  asm volatile("bar.sync %0, %1;" ::"r"(g + 1), "r"(THREADS) : "memory");
+}
+// Group barrier that also ANDs a flag over the group's threads, so that every
+// thread of the group takes the same branch after a bounded wait.
+__device__ __forceinline__ bool group_all(int g, bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\tsetp.ne.u32 p, %1, 0;\n\tbar.red.and.pred q, %2, %3, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v), "r"(g + 1), "r"(THREADS)
+      : "memory");
+  return r != 0;
+}
+
+// tile_gemm for one group: its 128 threads' shared-memory writes are fenced
+// and synced, its first thread issues the MMAs into the group's columns.
+__device__ __forceinline__ bool group_gemm(const __nv_bfloat16* a, const __nv_bfloat16* b, uint32_t tmem,
+                                           uint32_t mbar, uint32_t& parity, int g, int gt) {
+  fence_async_smem();
+  tc_fence_before();
+  group_sync(g);
+  tc_fence_after();
+  if (gt == 0) {
+    const uint32_t sa = smem_u32(a), sb = smem_u32(b);
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      mma_128x128x16(tmem, smem_desc(sa + k * 256, 128, 2048), smem_desc(sb + k * 256, 128, 2048), k > 0);
+    mma_commit(mbar);
+  }
+  const bool ok = group_all(g, mbar_wait(mbar, parity));
+  parity ^= 1u;
+  tc_fence_after();
+  return ok;
+}
+
+__global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, const float* __restrict__ x,
+                                                                float* __restrict__ out, int64_t n, int physical) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  __nv_bfloat16* act = reinterpret_cast<__nv_bfloat16*>(smem_raw);
-  __nv_bfloat16* w2 = act + TILE * H;
+  __nv_bfloat16* w2 = reinterpret_cast<__nv_bfloat16*>(smem_raw);
   __nv_bfloat16* w3 = w2 + TILE * H;
-  float* w1 = reinterpret_cast<float*>(w3 + TILE * H);
+  __nv_bfloat16* acts = w3 + TILE * H;  // kGroups activation tiles
+  float* w1 = reinterpret_cast<float*>(acts + kGroups * TILE * H);
   float* b1 = w1 + H * IN;
   float* b2 = b1 + H;
   float* b3 = b2 + H;
   float* w4 = b3 + H;
   float* b4 = w4 + OUT * H;
   float* nrm = b4 + 8;
-  uint64_t* mbar = reinterpret_cast<uint64_t*>(nrm + 24);
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbar + 1);
+  uint64_t* mbars = reinterpret_cast<uint64_t*>(nrm + 24);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(mbars + kGroups);
 
   const int t = threadIdx.x;
+  const int g = t >> 7, gt = t & (THREADS - 1);  // group, thread (= row) within the group
   load_tile(w2, P.w2tc);
   load_tile(w3, P.w3tc);
-  for (int i = t; i < H * IN; i += THREADS) w1[i] = P.w1r[i];
-  for (int i = t; i < OUT * H; i += THREADS) w4[i] = P.w4r[i];
-  for (int i = t; i < H; i += THREADS) {
+  for (int i = t; i < H * IN; i += INFER_THREADS) w1[i] = P.w1r[i];
+  for (int i = t; i < OUT * H; i += INFER_THREADS) w4[i] = P.w4r[i];
+  for (int i = t; i < H; i += INFER_THREADS) {
     b1[i] = P.p[OFF_B1 + i];
     b2[i] = P.p[OFF_B2 + i];
     b3[i] = P.p[OFF_B3 + i];
   }
   if (t < OUT) b4[t] = P.p[OFF_B4 + t];
   if (t < 18) nrm[t] = P.norm[t];
-  if (t == 0) mbar_init(smem_u32(mbar));
-  tmem_alloc(tslot);
+  if (t < kGroups) mbar_init(smem_u32(mbars + t));
+  if ((t >> 5) == 0) {  // all 512 columns: 128 per group
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tslot)));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  const uint32_t tmem = *tslot;
-  const uint32_t mb = smem_u32(mbar);
+  const uint32_t tmem_base = *tslot;
+  const uint32_t tmem = tmem_base + (uint32_t)(g * 128);           // the group's columns
+  const uint32_t taddr = tmem + ((uint32_t)(gt & ~31) << 16);      // this warp's 32 lanes
+  __nv_bfloat16* act = acts + g * TILE * H;
+  const uint32_t mb = smem_u32(mbars + g);
   uint32_t parity = 0;
   bool ok = true;
 
-  for (int64_t tile = blockIdx.x; ok && tile * TILE < n; tile += gridDim.x) {
-    const int64_t row = tile * TILE + t;
+  for (int64_t tile = (int64_t)blockIdx.x * kGroups + g; ok && tile * TILE < n; tile += (int64_t)gridDim.x * kGroups) {
+    const int64_t row = tile * TILE + gt;
     const bool valid = row < n;
     float xn[IN];
     float lnN = 0.f;
@@ -264,28 +318,28 @@ __global__ void __launch_bounds__(THREADS, 1) infer_kernel(DevParams P, const fl
         for (int j = 0; j < IN; ++j) z = fmaf(w1[f * IN + j], bf16r(xn[j]), z);
         v[i] = gelu_fast(z);
       }
-      store8(act, t, k8, v);
+      store8(act, gt, k8, v);
     }
     // layer 2 (tensor cores)
-    ok = tile_gemm(act, w2, tmem, mb, parity);
+    ok = group_gemm(act, w2, tmem, mb, parity, g, gt);
     if (!ok) break;
     for (int c = 0; c < 4; ++c) {
       float v[32];
-      tmem_ld32(lane_taddr(tmem) + c * 32, v);
+      tmem_ld32(taddr + c * 32, v);
 #pragma unroll
       for (int i = 0; i < 32; ++i) v[i] = gelu_fast(v[i] + b2[c * 32 + i]);
 #pragma unroll
-      for (int q = 0; q < 4; ++q) store8(act, t, c * 4 + q, v + q * 8);
+      for (int q = 0; q < 4; ++q) store8(act, gt, c * 4 + q, v + q * 8);
     }
     // layer 3 (tensor cores) and layer 4 (FP32 pipes), fused in the read-back
-    ok = tile_gemm(act, w3, tmem, mb, parity);
+    ok = group_gemm(act, w3, tmem, mb, parity, g, gt);
     if (!ok) break;
     float y[OUT];
 #pragma unroll
     for (int j = 0; j < OUT; ++j) y[j] = b4[j];
     for (int c = 0; c < 4; ++c) {
       float v[32];
-      tmem_ld32(lane_taddr(tmem) + c * 32, v);
+      tmem_ld32(taddr + c * 32, v);
 #pragma unroll
       for (int i = 0; i < 32; ++i) {
         const float h = bf16r(gelu_fast(v[i] + b3[c * 32 + i]));
@@ -306,11 +360,11 @@ __global__ void __launch_bounds__(THREADS, 1) infer_kernel(DevParams P, const fl
       }
     }
   }
-  if (!ok && t == 0) atomicExch(P.error, 1);
+  if (!ok && gt == 0) atomicExch(P.error, 1);
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
-  tmem_free(tmem);
+  if ((t >> 5) == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem_base));
 }
 
 // ---------------------------------------------------------------------------
@@ -711,7 +765,7 @@ __global__ void gamma_fit_kernel(const double* __restrict__ hist, int64_t n, int
   }
 }
 
-constexpr size_t kInferSmem = 3 * TILE_BYTES + (H * IN + 3 * H + OUT * H + 8 + 24) * 4 + 16 + 16;
+constexpr size_t kInferSmem = (2 + kGroups) * TILE_BYTES + (H * IN + 3 * H + OUT * H + 8 + 24) * 4 + 8 * kGroups + 16;
 constexpr size_t kTrainSmem = 3 * TILE_BYTES + (H * IN + OUT * H + 8 + TILE * OUT + 8) * 4 + 16 + 16;
 constexpr size_t kTestSmem = 2 * TILE_BYTES + 32;
 
@@ -907,8 +961,8 @@ pp_status pp_mlp_forward(pp_mlp* m, const float* d_x, float* d_out, int64_t n, i
   std::lock_guard<std::mutex> lk(m->mu);
   Guard g(m->device);
   const int64_t tiles = (n + mlp::TILE - 1) / mlp::TILE;
-  const int grid = (int)std::min<int64_t>(tiles, (int64_t)m->sm_count * 2);
-  mlp::infer_kernel<<<grid, mlp::THREADS, mlp::kInferSmem, static_cast<cudaStream_t>(stream)>>>(
+  const int grid = (int)std::min<int64_t>((tiles + mlp::kGroups - 1) / mlp::kGroups, (int64_t)m->sm_count);
+  mlp::infer_kernel<<<grid, mlp::INFER_THREADS, mlp::kInferSmem, static_cast<cudaStream_t>(stream)>>>(
       dev_params(m), d_x, d_out, n, physical);
   pp::count_launches(1);
   const cudaError_t e = cudaGetLastError();

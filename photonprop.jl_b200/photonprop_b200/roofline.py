@@ -14,8 +14,19 @@ per photon step   6 MUFU  (lg2 step length, rcp HG, sqrt sin(theta), sin, cos,
 per photon start  isotropic: 10 MUFU, 28 FP32; Cherenkov cone: 14 MUFU, 60 FP32;
                   plus one Philox block.
 A photon that hits the sphere also re-draws its emission block (rare).
+
+Two counts per photon step:
+  algorithmic (the reference's arithmetic, src/photon_prop_cuda.jl:319-361,
+  171-241: lg2 for the step length, rcp in the HG formula, sqrt of
+  1 - cos^2, sin and cos of the azimuth, sqrt of 1 - o_z^2, one rcp shared by
+  the two divisions by sin(theta), rsqrt to renormalise: 7 MUFU; about 45
+  FP32 operations) - the roofline's `achieved`;
+  issued (this kernel's form of the same step, counted above: 6 MUFU, 55
+  FP32) - reported beside it.
 """
 
+MUFU_PER_STEP_ALG = 7
+FP32_PER_STEP_ALG = 45
 MUFU_PER_STEP = 6
 FP32_PER_STEP = 55
 PHILOX_PER_STEP = 1
@@ -24,10 +35,13 @@ FP32_PER_PHOTON = {0: 28, 1: 60}
 PHILOX_PER_PHOTON = 1
 
 
-def op_counts(steps, photons_iso, photons_cone):
-    """(mufu, fp32, philox blocks) for a run."""
-    mufu = steps * MUFU_PER_STEP + photons_iso * MUFU_PER_PHOTON[0] + photons_cone * MUFU_PER_PHOTON[1]
-    fp32 = steps * FP32_PER_STEP + photons_iso * FP32_PER_PHOTON[0] + photons_cone * FP32_PER_PHOTON[1]
+def op_counts(steps, photons_iso, photons_cone, algorithmic=False):
+    """(mufu, fp32, philox blocks) for a run; algorithmic=True counts the
+    step as the reference's arithmetic does, else as this kernel issues it."""
+    m_step = MUFU_PER_STEP_ALG if algorithmic else MUFU_PER_STEP
+    f_step = FP32_PER_STEP_ALG if algorithmic else FP32_PER_STEP
+    mufu = steps * m_step + photons_iso * MUFU_PER_PHOTON[0] + photons_cone * MUFU_PER_PHOTON[1]
+    fp32 = steps * f_step + photons_iso * FP32_PER_PHOTON[0] + photons_cone * FP32_PER_PHOTON[1]
     blocks = steps * PHILOX_PER_STEP + (photons_iso + photons_cone) * PHILOX_PER_PHOTON
     return mufu, fp32, blocks
 
