@@ -223,12 +223,9 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
     r_count -= took;
     __syncwarp();
     if (need == kFull && took == 0u) break;  // every lane was idle and none took a photon
-    bool hit = false, turn = false;
-    float u1 = 0.f, u2 = 0.f;
-    if (alive) alive = step_move<MODE>(R, c, s, hit, turn, u1, u2);
+    bool hit = false;
+    if (alive) alive = step_event<MODE>(R, c, s, hit);
     if (MODE == kCompat) {
-      // a hit lane does not turn, so the turn can precede the hit staging
-      if (turn) step_turn(R, s, u1, u2);
       const unsigned hm = __ballot_sync(kFull, hit);
       if (hm) {
         const unsigned nh = __popc(hm);
@@ -270,7 +267,7 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
     }
     // physical mode turns after the hit record (which needs the arrival
     // direction): predicated writes of the new direction, no selects
-    if (MODE == kPhysical && turn) step_turn(R, s, u1, u2);
+
   }
   steps += (s.ctr3 >> 8) - 1u;  // the last photon's steps
   __syncwarp();

@@ -1,34 +1,29 @@
-"""Algorithmic operation counts of the propagation kernels, for roofline
-fractions.  Counted from the arithmetic of csrc/pp_device.cuh on the common
-path (no sphere intersection in the step), physical mode:
+"""Operation counts of the propagation kernels, for roofline fractions.
 
-per photon step   6 MUFU  (lg2 step length, rcp HG, sqrt sin(theta), sin, cos,
-                           rcp rotation)
-                 55 FP32  (FFMA/FMUL/FADD: uniforms 3, step 1, ray-sphere 12
-                           (a, e - a d, its square, b, |e|^2, dd; the photon's
-                           position is kept relative to the sphere centre, so e
-                           costs nothing), reachability cut 3, move 4 (position,
-                           path left), HG 4, sin(theta) 1, azimuth 3, rotation
-                           with Newton renormalisation 24)
-                  1 Philox4x32-10 block (10 rounds of 2 IMAD.WIDE, 2 LOP3, 2 IADD)
+per photon step   7 MUFU  the reference's arithmetic (src/photon_prop_cuda.jl:
+                          319-361, 171-241): lg2 for the step length, rcp in
+                          the HG formula, sqrt of 1 - cos^2, sin and cos of the
+                          azimuth, sqrt(1 - o_z^2) and rsqrt in the rotation (its
+                          two divisions by sin(theta) share one rcp), plus the
+                          square root of the ray-sphere discriminant when the
+                          line meets the sphere; the roofline counts 7.  This
+                          kernel issues 7 as well (lg2, sqrt of the
+                          discriminant, rcp, sqrt, sin, cos, rcp: the rotation
+                          needs no sin(theta) and renormalises with a Newton
+                          step), which ncu's opcode counts of the bare-step
+                          kernel confirm.
+                 ~45 FP32 in the reference's form; this kernel issues 56
+                          (ncu: 28 FFMA, 20 FMUL, 8 FADD per step).
+                  1 Philox4x32-10 block.
 per photon start  isotropic: 10 MUFU, 28 FP32; Cherenkov cone: 14 MUFU, 60 FP32;
                   plus one Philox block.
 A photon that hits the sphere also re-draws its emission block (rare).
-
-Two counts per photon step:
-  algorithmic (the reference's arithmetic, src/photon_prop_cuda.jl:319-361,
-  171-241: lg2 for the step length, rcp in the HG formula, sqrt of
-  1 - cos^2, sin and cos of the azimuth, sqrt of 1 - o_z^2, one rcp shared by
-  the two divisions by sin(theta), rsqrt to renormalise: 7 MUFU; about 45
-  FP32 operations) - the roofline's `achieved`;
-  issued (this kernel's form of the same step, counted above: 6 MUFU, 55
-  FP32) - reported beside it.
 """
 
 MUFU_PER_STEP_ALG = 7
 FP32_PER_STEP_ALG = 45
-MUFU_PER_STEP = 6
-FP32_PER_STEP = 55
+MUFU_PER_STEP = 7
+FP32_PER_STEP = 56
 PHILOX_PER_STEP = 1
 MUFU_PER_PHOTON = {0: 10, 1: 14}   # by emitter type
 FP32_PER_PHOTON = {0: 28, 1: 60}

@@ -109,7 +109,7 @@ def test_gamma_mixture_fit_recovers_parameters():
 
 def test_surrogate_trains_and_falls_back_to_mc(propagator, tmp_path):
     opts = pp.RunOptions(mode="physical", t_max=1000.0, hist_bins=1000)
-    train = sg.mc_dataset(propagator, sg.training_pairs(16384, 1_000_000, seed=11, d_min=2.0, d_max=10.0), opts)
+    train = sg.mc_dataset(propagator, sg.training_pairs(65536, 1_000_000, seed=11, d_min=2.0, d_max=10.0), opts)
     test = sg.mc_dataset(propagator, sg.training_pairs(1024, 1_000_000, seed=12, d_min=2.0, d_max=10.0), opts)
     s = sg.Surrogate(propagator, opts, seed=5)
     losses = s.fit(train, epochs=60, batch=1024, lr=2e-3)
@@ -120,12 +120,13 @@ def test_surrogate_trains_and_falls_back_to_mc(propagator, tmp_path):
         m = test.mask[:, j] > 0
         r2 = 1 - np.mean((raw[m, j] - test.y[m, j]) ** 2) / np.var(test.y[m, j])
         print("output", j, "held-out R^2", r2, "n", m.sum())
-    # expected hits on held-out pairs whose MC value is known to 3 %
+    # expected hits on held-out pairs whose MC value is known to 3 %: the
+    # network's median error against the MC is at most 5 %
     good = test.hits >= 1000
     pred = s.predict_features(test.x[good], physical=True)
     rel = np.abs(pred[:, 0] - test.mu[good]) / test.mu[good]
     print("pairs", good.sum(), "median rel err", np.median(rel), "within 5%", np.mean(rel < 0.05))
-    assert good.sum() > 50 and np.median(rel) < 0.10
+    assert good.sum() > 50 and np.median(rel) <= 0.05
     # the photon count scales the expected hits exactly
     x = test.x[good][:8].copy()
     x[:, 2] = 5.0
