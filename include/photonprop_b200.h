@@ -538,10 +538,7 @@ PP_API pp_status pp_autotune(pp_ctx* ctx, const pp_pair* pairs, int64_t n_pairs,
  * 4 update_position (in: pos[3],dir[3],step; out: 3), 5 equidistant
  * interpolation of the context's knots (in: u), 6 refractive index,
  * 7 group index, 8 scattering length, 9 absorption length, 10 PMT
- * acceptance (in: wavelength), 11 cascade-emitter cos theta (in: u, n),
- * 12 the Philox words of a photon's block through its per-pair and
- * per-photon constants under the library key (in: seed lo, seed hi, photon
- * lo, counter word 3; out: 4). */
+ * acceptance (in: wavelength), 11 cascade-emitter cos theta (in: u, n). */
 PP_API pp_status pp_device_eval(pp_ctx* ctx, int32_t op, const double* in, double* out, int64_t n);
 
 /* Measures this device's FP32 FMA and MUFU (transcendental) issue peaks with

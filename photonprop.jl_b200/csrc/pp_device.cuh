@@ -71,17 +71,27 @@ __device__ __forceinline__ float cos_a(float x) {
 }
 
 // ---- Philox4x32-10 (Salmon et al., SC'11) ---------------------------------
+// Each round's products are written as a 32-bit high half (__umulhi) and a
+// 32-bit low product rather than as one 64-bit product: the same numbers,
+// but on sm_100a the 64-bit form cost two extra integer adds per round on the
+// half-rate ALU pipe (ncu opcode counts of the bare step); this form ran the
+// bare step 16 % and the batched kernel 10 % faster.
 __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
-    const uint64_t p0 = (uint64_t)c[0] * 0xD2511F53u;
-    const uint64_t p1 = (uint64_t)c[2] * 0xCD9E8D57u;
-    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ k0;
-    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ k1;
+#ifdef __CUDA_ARCH__
+    const uint32_t h0 = __umulhi(c[0], 0xD2511F53u), l0 = c[0] * 0xD2511F53u;
+    const uint32_t h1 = __umulhi(c[2], 0xCD9E8D57u), l1 = c[2] * 0xCD9E8D57u;
+#else
+    const uint64_t p0 = (uint64_t)c[0] * 0xD2511F53u, p1 = (uint64_t)c[2] * 0xCD9E8D57u;
+    const uint32_t h0 = (uint32_t)(p0 >> 32), l0 = (uint32_t)p0, h1 = (uint32_t)(p1 >> 32), l1 = (uint32_t)p1;
+#endif
+    const uint32_t n0 = h1 ^ c[1] ^ k0;
+    const uint32_t n2 = h0 ^ c[3] ^ k1;
     c[0] = n0;
-    c[1] = (uint32_t)p1;
+    c[1] = l1;
     c[2] = n2;
-    c[3] = (uint32_t)p0;
+    c[3] = l0;
     k0 += 0x9E3779B9u;
     k1 += 0xBB67AE85u;
   }
@@ -112,75 +122,6 @@ __device__ __forceinline__ uint32_t ctr_word(uint64_t photon, uint32_t block) {
 __device__ __forceinline__ Draw4 draw_block(uint32_t seed_lo, uint32_t seed_hi, uint64_t photon, uint32_t word3) {
   uint32_t c[4] = {seed_lo, seed_hi, (uint32_t)photon, word3};
   philox4x32_10(c, kKey0, kKey1);
-  return Draw4{u01(c[0]), u01(c[1]), u01(c[2]), u01(c[3])};
-}
-
-// A photon's counter words 0..2 (seed lo, seed hi, photon lo) never change,
-// so with the key fixed the first Philox round depends on the block only
-// through word 3, and the second round's products of words that came from
-// words 0..2 are fixed too.  Per step, rounds 1-2 then reduce to one XOR, one
-// 32 x 32 -> 64 multiply and one XOR, given one constant per pair (pc) and
-// three per photon (pb, pe, pf); rounds 3-10 run as usual.  The numbers are
-// exactly those of philox4x32_10 on the full counter.
-__host__ __device__ __forceinline__ uint32_t mulhi32(uint32_t a, uint32_t b) {
-  return (uint32_t)(((uint64_t)a * b) >> 32);
-}
-constexpr uint32_t kM0 = 0xD2511F53u, kM1 = 0xCD9E8D57u;  // Philox4x32 multipliers
-constexpr uint32_t kW0 = 0x9E3779B9u, kW1 = 0xBB67AE85u;  // Weyl key increments
-
-// The products are written as a 32-bit high half (__umulhi) and a 32-bit
-// low product rather than one 64-bit product: the same numbers, but the
-// 64-bit form cost extra integer instructions per round on sm_100a (the bare
-// step ran 11 % faster, the batched kernel 6 %, when this form replaced it).
-template <int R0>
-__host__ __device__ __forceinline__ void philox_rounds_from(uint32_t c[4]) {
-#pragma unroll
-  for (int r = R0; r < 10; ++r) {
-    const uint32_t k0 = kKey0 + (uint32_t)r * kW0, k1 = kKey1 + (uint32_t)r * kW1;
-#ifdef __CUDA_ARCH__
-    const uint32_t h0 = __umulhi(c[0], kM0), l0 = c[0] * kM0;
-    const uint32_t h1 = __umulhi(c[2], kM1), l1 = c[2] * kM1;
-#else
-    const uint64_t p0 = (uint64_t)c[0] * kM0, p1 = (uint64_t)c[2] * kM1;
-    const uint32_t h0 = (uint32_t)(p0 >> 32), l0 = (uint32_t)p0, h1 = (uint32_t)(p1 >> 32), l1 = (uint32_t)p1;
-#endif
-    const uint32_t n0 = h1 ^ c[1] ^ k0;
-    const uint32_t n2 = h0 ^ c[3] ^ k1;
-    c[0] = n0;
-    c[1] = l1;
-    c[2] = n2;
-    c[3] = l0;
-  }
-}
-
-__host__ __device__ __forceinline__ uint32_t philox_pair_const(uint32_t seed_lo) {
-  return mulhi32(seed_lo, kM0) ^ kKey1;
-}
-struct PhiloxPhoton {
-  uint32_t b, e, f;
-};
-__host__ __device__ __forceinline__ PhiloxPhoton philox_photon_consts(uint32_t seed_lo, uint32_t seed_hi,
-                                                                     uint32_t photon_lo) {
-  const uint32_t a = mulhi32(photon_lo, kM1) ^ seed_hi ^ kKey0;
-  PhiloxPhoton k;
-  k.b = photon_lo * kM1;
-  k.e = mulhi32(a, kM0) ^ (seed_lo * kM0) ^ (kKey1 + kW1);
-  k.f = a * kM0;
-  return k;
-}
-// The four output words of block word3 of a photon, from its constants.
-__host__ __device__ __forceinline__ void philox_words(uint32_t pc, uint32_t pb, uint32_t pe, uint32_t pf,
-                                                     uint32_t word3, uint32_t c[4]) {
-  const uint64_t p1 = (uint64_t)(pc ^ word3) * kM1;
-  c[0] = (uint32_t)(p1 >> 32) ^ pb ^ (kKey0 + kW0);
-  c[1] = (uint32_t)p1;
-  c[2] = pe;
-  c[3] = pf;
-  philox_rounds_from<2>(c);
-}
-__device__ __forceinline__ Draw4 draw_pre(uint32_t pc, uint32_t pb, uint32_t pe, uint32_t pf, uint32_t word3) {
-  uint32_t c[4];
-  philox_words(pc, pb, pe, pf, word3, c);
   return Draw4{u01(c[0]), u01(c[1]), u01(c[2]), u01(c[3])};
 }
 
@@ -347,42 +288,23 @@ struct Photon {
   float path;         // physical: path left before t_max; compat: path travelled
   float neg_ln2_len;  // -ln2 * scattering length: step = lg2(u) * this
   uint32_t ctr3;      // Philox counter word of the next event: block (= steps + 1) << 8 | photon bits 32..39
-  uint32_t id_lo;     // photon index bits 0..31
-  uint32_t pb, pe, pf;  // the photon's Philox constants (philox_photon_consts)
+  uint64_t id;
 };
 
-__device__ __forceinline__ uint64_t photon_index(const Photon& s) {
-  return ((uint64_t)(s.ctr3 & 0xFFu) << 32) | s.id_lo;
-}
-
 struct PairCtx {
-  float r;       // sphere radius
-  uint32_t pc;   // the pair's Philox constant (philox_pair_const of its seed)
+  float r;  // sphere radius
+  uint32_t seed_lo, seed_hi;
   int32_t index;
 };
 
-__device__ __forceinline__ uint2 pair_seed(const pp_pair* __restrict__ P) {
-  return __ldg(reinterpret_cast<const uint2*>(P) + 7);
-}
-
 __device__ __forceinline__ PairCtx load_pair_ctx(const pp_pair* __restrict__ P, int index) {
+  const uint2 sd = __ldg(reinterpret_cast<const uint2*>(P) + 7);  // seed
   PairCtx c;
   c.r = __ldg(reinterpret_cast<const float*>(P) + 11);  // radius
-  c.pc = philox_pair_const(pair_seed(P).x);
+  c.seed_lo = sd.x;
+  c.seed_hi = sd.y;
   c.index = index;
   return c;
-}
-
-// Sets photon `photon` of pair P up for its emission: index words, Philox
-// constants and the counter word of block 0.
-__device__ __forceinline__ void photon_start(const pp_pair* __restrict__ P, uint64_t photon, Photon& s) {
-  const uint2 sd = pair_seed(P);
-  const PhiloxPhoton k = philox_photon_consts(sd.x, sd.y, (uint32_t)photon);
-  s.id_lo = (uint32_t)photon;
-  s.pb = k.b;
-  s.pe = k.e;
-  s.pf = k.f;
-  s.ctr3 = ctr_word(photon, 0u);
 }
 
 __device__ __forceinline__ float3 pair_target(const pp_pair* __restrict__ P) {
@@ -493,13 +415,12 @@ __device__ __forceinline__ float path_at_tmax(const DevTables& T, const RunParam
   return (R.t_max - f.t_emit) * kCVac * rcp(group_index(T, rcp(f.wl)));
 }
 
-// Emission of the photon set up by photon_start (block 0): position,
-// direction and the per-wavelength constants; afterwards the next event is
-// block 1.
+// Emission of photon s.id (block 0): position, direction and the
+// per-wavelength constants; afterwards the next event is block 1.
 template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                            const PairCtx& c, Photon& s) {
-  const Draw4 d = draw_pre(c.pc, s.pb, s.pe, s.pf, s.ctr3 & 0xFFu);
+  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, ctr_word(s.id, 0u));
   const EmissionFrame f = emission_frame<MODE, EM>(T, P, d);
   const float3 tg = pair_target(P);
   s.px = f.px - tg.x;
@@ -508,18 +429,16 @@ __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& 
   s.path = (MODE == kPhysical) ? path_at_tmax(T, R, f) : 0.f;
   s.neg_ln2_len = -kLn2 * scattering_length(T, f.wl);
   emission_direction(f, d.u2, s.dx, s.dy, s.dz);
-  s.ctr3 = (s.ctr3 & 0xFFu) | (1u << 8);
+  s.ctr3 = ctr_word(s.id, 1u);
 }
 
-// Step k (block k + 1) of src/photon_prop_cuda.jl:320-376, first half: step
-// length, ray-sphere test and move.  Returns false when the photon ends;
-// *hit is set when it ends on the sphere (position and path length then at
-// the hit, direction the arrival direction), *turn when the step's
-// Henyey-Greenstein turn applies, with the turn's uniforms in u1, u2.
+// Step k (block k + 1) of src/photon_prop_cuda.jl:320-376: step length,
+// ray-sphere test, move, Henyey-Greenstein turn.  Returns false when the
+// photon ends; *hit is set when it ends on the sphere (position and path
+// length then at the hit).
 template <int MODE>
-__device__ __forceinline__ bool step_move(const RunParams& R, const PairCtx& c, Photon& s, bool& hit, bool& turn,
-                                          float& u1, float& u2) {
-  const Draw4 d = draw_pre(c.pc, s.pb, s.pe, s.pf, s.ctr3);
+__device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c, Photon& s, bool& hit) {
+  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, s.ctr3);
   const float step = lg2(d.u0) * s.neg_ln2_len;
   const float ex = s.px, ey = s.py, ez = s.pz;  // photon - sphere centre
   const float a = fmaf(s.dz, ez, fmaf(s.dy, ey, s.dx * ex));
@@ -530,18 +449,16 @@ __device__ __forceinline__ bool step_move(const RunParams& R, const PairCtx& c, 
   const float q = fmaf(qz, qz, fmaf(qy, qy, qx * qx));
   const float b = fmaf(c.r, c.r, -q);
   const float pp = fmaf(a, a, q);  // |e|^2
-  // the line meets the sphere at dd ahead (b < 0: the approximate square root
-  // of a negative number is NaN, so dd is NaN and every comparison below is
-  // false: no intersection)
+  // branch-free decisions: the line meets the sphere (b >= 0) at dd ahead
+  // (b < 0 makes dd NaN, which no decision reads: line is false)
   const float dd = -a - sqrt_a(b);
-  const bool geo = dd > 0.f && dd < step;  // reaches the sphere within this step
+  const bool line = b >= 0.f;
+  const bool geo = line && dd > 0.f && dd < step;  // reaches the sphere within this step
   bool alive, move;
-  float len;
   if (MODE == kCompat) {
     hit = geo;
-    move = !(b >= 0.f);  // the line meets the sphere outside this step: no move (reference)
+    move = !line;  // the line meets the sphere outside this step: no move (reference)
     alive = !geo;
-    len = hit ? dd : (move ? step : 0.f);
   } else {
     hit = geo && dd <= s.path;  // arrives inside the time window
     // A photon farther from the sphere than the path it has left before t_max
@@ -551,35 +468,20 @@ __device__ __forceinline__ bool step_move(const RunParams& R, const PairCtx& c, 
     const float reach = fmaf(s.path, 1.0001f, c.r + 0.05f);
     move = !geo && step <= s.path && pp <= reach * reach;
     alive = move;
-    len = geo ? dd : step;  // a photon that ends without a hit keeps no state
   }
+  const float len = hit ? dd : (move ? step : 0.f);
   s.px = fmaf(len, s.dx, s.px);
   s.py = fmaf(len, s.dy, s.py);
   s.pz = fmaf(len, s.dz, s.pz);
   s.path += (MODE == kPhysical) ? -len : len;
-  s.ctr3 += 1u << 8;
-  turn = move;
-  u1 = d.u1;
-  u2 = d.u2;
-  return alive && s.ctr3 < R.ctr_limit;  // at most max_steps steps
-}
-
-// The whole step: the move, then the Henyey-Greenstein turn
-// (src/photon_prop_cuda.jl:223-241 via update_direction), computed on every
-// lane and kept by a select where it applies (a branch around it costs the
-// warp more than the three selects, and a hit keeps its arrival direction).
-template <int MODE>
-__device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c, Photon& s, bool& hit) {
-  bool turn;
-  float u1, u2;
-  const bool alive = step_move<MODE>(R, c, s, hit, turn, u1, u2);
-  const float cpol = hg_costheta(R.hg, u1);
+  const float cpol = hg_costheta(R.hg, d.u1);
   float rx, ry, rz;
-  polar_direction<false>(s.dx, s.dy, s.dz, cpol, sin_from_cos(cpol), u2, rx, ry, rz);
-  s.dx = turn ? rx : s.dx;
-  s.dy = turn ? ry : s.dy;
-  s.dz = turn ? rz : s.dz;
-  return alive;
+  polar_direction<false>(s.dx, s.dy, s.dz, cpol, sin_from_cos(cpol), d.u2, rx, ry, rz);
+  s.dx = move ? rx : s.dx;
+  s.dy = move ? ry : s.dy;
+  s.dz = move ? rz : s.dz;
+  s.ctr3 += 1u << 8;
+  return alive && s.ctr3 < R.ctr_limit;  // at most max_steps steps
 }
 
 // Emission (block 0) or step event of one photon.
@@ -605,7 +507,7 @@ struct HitValues {
 template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ HitValues hit_values(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                                 const PairCtx& c, const Photon& s) {
-  const Draw4 d = draw_pre(c.pc, s.pb, s.pe, s.pf, s.ctr3 & 0xFFu);
+  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, ctr_word(s.id, 0u));
   const EmissionFrame f = emission_frame<MODE, EM>(T, P, d);
   HitValues h;
   h.wl = f.wl;
@@ -644,7 +546,7 @@ __device__ __forceinline__ void write_hit(const RunParams& R, const PairCtx& c, 
     if (R.flags & PP_OPT_COMPACT_HITS) {
       float4* dst = reinterpret_cast<float4*>(reinterpret_cast<pp_hit32*>(R.hits) + idx);
       dst[0] = make_float4(h.px, h.py, h.pz, h.time);
-      dst[1] = make_float4(h.weight, h.wl, __uint_as_float(s.id_lo),
+      dst[1] = make_float4(h.weight, h.wl, __uint_as_float((uint32_t)s.id),
                            __uint_as_float((uint32_t)c.index + R.pair_base));
     } else {
       float4* dst = reinterpret_cast<float4*>(R.hits + idx);
@@ -652,7 +554,7 @@ __device__ __forceinline__ void write_hit(const RunParams& R, const PairCtx& c, 
       dst[1] = make_float4(h.d0x, h.d0y, h.d0z, h.weight);
       dst[2] = make_float4(s.dx, s.dy, s.dz, h.wl);
       dst[3] = make_float4(h.dist, __uint_as_float((uint32_t)c.index + R.pair_base),
-                           __uint_as_float(s.id_lo), __uint_as_float(s.ctr3 & 0xFFu));
+                           __uint_as_float((uint32_t)s.id), __uint_as_float((uint32_t)(s.id >> 32)));
     }
   } else {
     atomicOr(R.counters + 2, 1ull);

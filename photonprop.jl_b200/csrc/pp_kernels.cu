@@ -34,10 +34,11 @@ constexpr int kStage = 64;  // >= 2 * 32 - 1 staged emissions per warp (power of
 
 struct __align__(16) Staged {
   float px, py, pz, dx, dy, dz, neg_ln2_len, path;
-  uint32_t id_lo, ctr3;
+  uint32_t id_lo, id_hi;
   int32_t pair;
-  float radius;            // the pair's sphere radius and Philox constant, so
-  uint32_t pb, pe, pf, pc;  // that a refill reads shared memory only
+  float radius;              // the pair's sphere radius and seed, so that a
+  uint32_t seed_lo, seed_hi;  // refill reads shared memory only
+  uint32_t pad[2];
 };
 
 // Compat mode hits often: a photon whose line meets the sphere beyond its
@@ -64,9 +65,6 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
   __shared__ Staged stage[WARPS][kStage];
   __shared__ WarpStats wstats[WARPS];
   __shared__ StagedHit hstage[MODE == kCompat ? WARPS : 1][kHitStage];
-  // the lane's photon index (bits 0..31) and pair index: needed only to
-  // record a hit, so they wait here instead of in registers through the steps
-  __shared__ uint2 lane_ids[WARPS * 32];
   stage_tables(T, R.tables);
   if ((threadIdx.x & 31u) == 0) {
     WarpStats& w0 = wstats[threadIdx.x >> 5];
@@ -95,7 +93,8 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
       p.dz = g.dz;
       p.path = g.path;
       p.neg_ln2_len = 0.f;
-      photon_start(R.pairs + g.pair, ((unsigned long long)g.id_hi << 32) | g.id_lo, p);
+      p.id = ((unsigned long long)g.id_hi << 32) | g.id_lo;
+      p.ctr3 = 0u;
       const PairCtx pc = load_pair_ctx(R.pairs + g.pair, g.pair);
       const HitValues h = hit_values<MODE, EM>(T, R, R.pairs + g.pair, pc, p);
       record_hit_cached(R, ws, pc, p, h);
@@ -113,14 +112,13 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
   // lane state
   bool alive = false;
   Photon s;
-  s.id_lo = 0u;
-  s.pb = s.pe = s.pf = 0u;
+  s.id = 0;
   s.ctr3 = 1u << 8;
   s.px = s.py = s.pz = s.dx = s.dy = s.path = s.neg_ln2_len = 0.f;
   s.dz = 1.f;
   PairCtx c;
   c.r = 0.f;
-  c.pc = 0u;
+  c.seed_lo = c.seed_hi = 0u;
   c.index = 0;
   unsigned steps = 0;
 
@@ -182,14 +180,14 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         const pp_pair* P = R.pairs + ppair;
         const PairCtx pc = load_pair_ctx(P, ppair);
         Photon e;
-        photon_start(P, pid, e);
+        e.id = pid;
         emit_event<MODE, EM>(T, R, P, pc, e);
         float4* dst = reinterpret_cast<float4*>(ring + ((r_head + r_count + lane) & (kStage - 1)));
         dst[0] = make_float4(e.px, e.py, e.pz, e.dx);
         dst[1] = make_float4(e.dy, e.dz, e.neg_ln2_len, e.path);
-        dst[2] = make_float4(__uint_as_float(e.id_lo), __uint_as_float(e.ctr3), __int_as_float(ppair), pc.r);
-        dst[3] = make_float4(__uint_as_float(e.pb), __uint_as_float(e.pe), __uint_as_float(e.pf),
-                             __uint_as_float(pc.pc));
+        dst[2] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)),
+                             __int_as_float(ppair), pc.r);
+        dst[3] = make_float4(__uint_as_float(pc.seed_lo), __uint_as_float(pc.seed_hi), 0.f, 0.f);
       }
       r_count += filled;
       __syncwarp();
@@ -197,7 +195,6 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
     if (!alive) {
       const unsigned rank = __popc(need & lt_mask);
       if (rank < r_count) {
-        steps += (s.ctr3 >> 8) - 1u;  // the ended photon's steps (block = steps + 1)
         const float4* src = reinterpret_cast<const float4*>(ring + ((r_head + rank) & (kStage - 1)));
         const float4 a = src[0], b = src[1], d = src[2], e = src[3];
         s.px = a.x;
@@ -208,13 +205,12 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         s.dz = b.y;
         s.neg_ln2_len = b.z;
         s.path = b.w;
-        lane_ids[threadIdx.x] = make_uint2(__float_as_uint(d.x), __float_as_uint(d.z));
-        s.ctr3 = __float_as_uint(d.y);
+        s.id = ((unsigned long long)__float_as_uint(d.y) << 32) | __float_as_uint(d.x);
+        s.ctr3 = ctr_word(s.id, 1u);
+        c.index = __float_as_int(d.z);
         c.r = d.w;
-        s.pb = __float_as_uint(e.x);
-        s.pe = __float_as_uint(e.y);
-        s.pf = __float_as_uint(e.z);
-        c.pc = __float_as_uint(e.w);
+        c.seed_lo = __float_as_uint(e.x);
+        c.seed_hi = __float_as_uint(e.y);
         alive = true;
       }
     }
@@ -224,7 +220,10 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
     __syncwarp();
     if (need == kFull && took == 0u) break;  // every lane was idle and none took a photon
     bool hit = false;
-    if (alive) alive = step_event<MODE>(R, c, s, hit);
+    if (alive) {
+      ++steps;
+      alive = step_event<MODE>(R, c, s, hit);
+    }
     if (MODE == kCompat) {
       const unsigned hm = __ballot_sync(kFull, hit);
       if (hm) {
@@ -234,9 +233,6 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
           h_count = 0;
         }
         if (hit) {
-          const uint2 ids = lane_ids[threadIdx.x];
-          s.id_lo = ids.x;
-          c.index = (int)ids.y;
           StagedHit& g = hst[h_count + __popc(hm & lt_mask)];
           g.px = s.px;
           g.py = s.py;
@@ -245,8 +241,8 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
           g.dy = s.dy;
           g.dz = s.dz;
           g.path = s.path;
-          g.id_lo = s.id_lo;
-          g.id_hi = s.ctr3 & 0xFFu;
+          g.id_lo = (uint32_t)s.id;
+          g.id_hi = (uint32_t)(s.id >> 32);
           g.pair = c.index;
         }
         h_count += nh;
@@ -258,18 +254,11 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
       }
     } else if (__any_sync(kFull, hit)) {
       if (hit) {
-        const uint2 ids = lane_ids[threadIdx.x];
-        s.id_lo = ids.x;
-        c.index = (int)ids.y;
         const HitValues h = hit_values<MODE, EM>(T, R, R.pairs + c.index, c, s);
         record_hit_cached(R, ws, c, s, h);
       }
     }
-    // physical mode turns after the hit record (which needs the arrival
-    // direction): predicated writes of the new direction, no selects
-
   }
-  steps += (s.ctr3 >> 8) - 1u;  // the last photon's steps
   __syncwarp();
   if (MODE == kCompat && h_count > 0u) record_staged(h_count);
   if (lane == 0) flush_warp_stats(R.stats, ws);
@@ -295,7 +284,8 @@ __global__ void __launch_bounds__(512) plain_kernel(const RunParams R, const pp_
   for (unsigned long long id = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; id < n;
        id += stride) {
     Photon s;
-    photon_start(pair_ptr, id, s);
+    s.id = id;
+    s.ctr3 = ctr_word(id, 0u);
     s.dx = s.dy = 0.f;
     s.dz = 1.f;
     bool alive = true;
@@ -340,7 +330,8 @@ __global__ void __launch_bounds__(1024) stacks_kernel(const RunParams R, const p
   for (long long i = 0; i < per_thread; ++i) {
     if (*(volatile int*)&cursor > ix_offset + stack_len - safe_margin) break;
     Photon s;
-    photon_start(pair_ptr, g + (unsigned long long)i * G, s);
+    s.id = g + (unsigned long long)i * G;
+    s.ctr3 = ctr_word(s.id, 0u);
     s.dx = s.dy = 0.f;
     s.dz = 1.f;
     bool alive = true;
@@ -497,15 +488,6 @@ __global__ void eval_kernel(int op, const double* __restrict__ in, double* __res
     case 10:
       out[i] = T.n_pmt > 0 ? (double)interp_sorted((float)in[i], T.pmt_wl, T.pmt_acc, T.n_pmt) : 1.0;
       break;
-    case 12: {  // Philox words through the per-pair/per-photon constants (fixed library key)
-      const double* a = in + 4 * i;
-      const uint32_t seed_lo = (uint32_t)a[0], seed_hi = (uint32_t)a[1], photon_lo = (uint32_t)a[2];
-      const PhiloxPhoton k = philox_photon_consts(seed_lo, seed_hi, photon_lo);
-      uint32_t c[4];
-      philox_words(philox_pair_const(seed_lo), k.b, k.e, k.f, (uint32_t)a[3], c);
-      for (int j = 0; j < 4; ++j) out[4 * i + j] = (double)c[j];
-      break;
-    }
     default: out[i] = 0.0;
   }
 }
@@ -563,16 +545,11 @@ __global__ void __launch_bounds__(256, 4) peak_step_kernel(const RunParams R, in
                                                            unsigned long long* __restrict__ out) {
   PairCtx c;
   c.r = 0.21f;
-  const uint32_t seed_lo = 0x9E3779B9u * (blockIdx.x + 1u), seed_hi = 0x2545F491u;
-  c.pc = philox_pair_const(seed_lo);
+  c.seed_lo = 0x9E3779B9u * (blockIdx.x + 1u);
+  c.seed_hi = 0x2545F491u;
   c.index = 0;
   Photon s;
-  const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const PhiloxPhoton k = philox_photon_consts(seed_lo, seed_hi, (uint32_t)id);
-  s.id_lo = (uint32_t)id;
-  s.pb = k.b;
-  s.pe = k.e;
-  s.pf = k.f;
+  s.id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   s.px = 100.f + (float)(threadIdx.x & 31u);
   s.py = 50.f;
   s.pz = -30.f;
@@ -581,7 +558,7 @@ __global__ void __launch_bounds__(256, 4) peak_step_kernel(const RunParams R, in
   s.dz = 0.8f;
   s.path = 1e30f;
   s.neg_ln2_len = -kLn2 * 30.f;
-  s.ctr3 = ctr_word(id, 1u);
+  s.ctr3 = ctr_word(s.id, 1u);
   unsigned live = 0;
   for (int i = 0; i < iters; ++i) {
     bool hit = false;

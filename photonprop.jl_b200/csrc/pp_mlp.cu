@@ -54,7 +54,14 @@ __device__ __forceinline__ float gelu(float z) {
   return 0.5f * z * (1.f + tanhf(u));
 }
 // Inference GELU with the MUFU tanh (tanh.approx.f32, relative error below
-// 2^-10, under the BF16 rounding that follows it).
+// 2^-10, under the BF16 rounding that follows it), in five FP32 operations:
+// u = z (k + k c z^2), GELU = z (1/2 + t/2).
+__device__ __forceinline__ float gelu_fast5(float z) {
+  const float u = z * fmaf(0.7978845608028654f * 0.044715f, z * z, 0.7978845608028654f);
+  float t;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
+  return z * fmaf(0.5f, t, 0.5f);
+}
 __device__ __forceinline__ float gelu_fast(float z) {
   const float u = 0.7978845608028654f * fmaf(0.044715f * z, z * z, z);
   float t;
@@ -177,6 +184,31 @@ __device__ __forceinline__ bool tile_gemm(const __nv_bfloat16* a, const __nv_bfl
   return ok;
 }
 
+// element offset of (row, k) in a K-major canonical tile of 16 columns
+__host__ __device__ __forceinline__ int tc16_offset(int row, int k) {
+  return (((row >> 3) * 2 + (k >> 3)) << 6) + ((row & 7) << 3) + (k & 7);
+}
+// Instruction descriptor for N = 16 (the padded output layer).
+constexpr uint32_t kIdescN16 = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+__device__ __forceinline__ void mma_idesc(uint32_t tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+// 16 FP32 accumulator columns [col, col+16) of this thread's row.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 __device__ __forceinline__ uint32_t lane_taddr(uint32_t tmem) { return tmem + ((threadIdx.x & ~31u) << 16); }
 
 // ---------------------------------------------------------------------------
@@ -187,6 +219,8 @@ struct DevParams {
   const float* w4r;      // BF16-rounded W4 [5][128]
   const __nv_bfloat16* w2tc;   // W2 as the B operand of h W2^T (canonical tile)
   const __nv_bfloat16* w3tc;
+  const __nv_bfloat16* w1tc;   // W1 as the B operand of x W1^T: 128 rows x K 16 (4 used)
+  const __nv_bfloat16* w4tc;   // W4 as the B operand of h W4^T: 16 rows (5 used) x K 128
   const __nv_bfloat16* w2ttc;  // W2^T as the B operand of dz W2
   const __nv_bfloat16* w3ttc;
   const float* norm;     // x_mean[4], x_std[4], y_mean[5], y_std[5]
@@ -251,18 +285,44 @@ __device__ __forceinline__ bool group_gemm(const __nv_bfloat16* a, const __nv_bf
   return ok;
 }
 
+// The group's MMAs of one layer; kind 1: x (128 x 16) W1^T, one MMA;
+// kind 2: h (128 x 128) W^T, eight MMAs; kind 4: h W4^T with N = 16.
+__device__ __forceinline__ bool group_layer(int kind, const __nv_bfloat16* a, const __nv_bfloat16* b, uint32_t tmem,
+                                            uint32_t mbar, uint32_t& parity, int g, int gt) {
+  fence_async_smem();
+  tc_fence_before();
+  group_sync(g);
+  tc_fence_after();
+  if (gt == 0) {
+    const uint32_t sa = smem_u32(a), sb = smem_u32(b);
+    if (kind == 1) {
+      mma_idesc(tmem, smem_desc(sa, 128, 256), smem_desc(sb, 128, 256), kIdesc, 0u);
+    } else {
+      const uint32_t idesc = kind == 4 ? kIdescN16 : kIdesc;
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+        mma_idesc(tmem, smem_desc(sa + k * 256, 128, 2048), smem_desc(sb + k * 256, 128, 2048), idesc, k > 0);
+    }
+    mma_commit(mbar);
+  }
+  const bool ok = group_all(g, mbar_wait(mbar, parity));
+  parity ^= 1u;
+  tc_fence_after();
+  return ok;
+}
+
 __global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, const float* __restrict__ x,
                                                                 float* __restrict__ out, int64_t n, int physical) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __nv_bfloat16* w2 = reinterpret_cast<__nv_bfloat16*>(smem_raw);
   __nv_bfloat16* w3 = w2 + TILE * H;
-  __nv_bfloat16* acts = w3 + TILE * H;  // kGroups activation tiles
-  float* w1 = reinterpret_cast<float*>(acts + kGroups * TILE * H);
-  float* b1 = w1 + H * IN;
+  __nv_bfloat16* w1t = w3 + TILE * H;   // 128 x 16
+  __nv_bfloat16* w4t = w1t + H * 16;    // 16 x 128
+  __nv_bfloat16* acts = w4t + 16 * H;   // kGroups activation tiles (the x tile is the first 4 KB of one)
+  float* b1 = reinterpret_cast<float*>(acts + kGroups * TILE * H);
   float* b2 = b1 + H;
   float* b3 = b2 + H;
-  float* w4 = b3 + H;
-  float* b4 = w4 + OUT * H;
+  float* b4 = b3 + H;
   float* nrm = b4 + 8;
   uint64_t* mbars = reinterpret_cast<uint64_t*>(nrm + 24);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbars + kGroups);
@@ -271,8 +331,11 @@ __global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, co
   const int g = t >> 7, gt = t & (THREADS - 1);  // group, thread (= row) within the group
   load_tile(w2, P.w2tc);
   load_tile(w3, P.w3tc);
-  for (int i = t; i < H * IN; i += INFER_THREADS) w1[i] = P.w1r[i];
-  for (int i = t; i < OUT * H; i += INFER_THREADS) w4[i] = P.w4r[i];
+  {
+    const int4* s1 = reinterpret_cast<const int4*>(P.w1tc);
+    int4* d1 = reinterpret_cast<int4*>(w1t);
+    for (int i = t; i < 2 * H * 16 * 2 / 16; i += INFER_THREADS) d1[i] = s1[i];  // both 4 KB tiles
+  }
   for (int i = t; i < H; i += INFER_THREADS) {
     b1[i] = P.p[OFF_B1 + i];
     b2[i] = P.p[OFF_B2 + i];
@@ -299,7 +362,7 @@ __global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, co
   for (int64_t tile = (int64_t)blockIdx.x * kGroups + g; ok && tile * TILE < n; tile += (int64_t)gridDim.x * kGroups) {
     const int64_t row = tile * TILE + gt;
     const bool valid = row < n;
-    float xn[IN];
+    float xn[8];
     float lnN = 0.f;
 #pragma unroll
     for (int j = 0; j < IN; ++j) {
@@ -307,50 +370,57 @@ __global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, co
       if (j == 2) lnN = raw * 2.302585092994046f;
       xn[j] = (raw - nrm[j]) / nrm[4 + j];
     }
-    // layer 1 (FP32 pipes)
-    for (int k8 = 0; k8 < H / 8; ++k8) {
-      float v[8];
 #pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const int f = k8 * 8 + i;
-        float z = b1[f];
+    for (int j = IN; j < 8; ++j) xn[j] = 0.f;
+    // layer 1 (tensor cores, K = 4 padded to 16): the row's x in the x tile
+    {
+      __align__(16) __nv_bfloat162 p[4];
 #pragma unroll
-        for (int j = 0; j < IN; ++j) z = fmaf(w1[f * IN + j], bf16r(xn[j]), z);
-        v[i] = gelu_fast(z);
-      }
-      store8(act, gt, k8, v);
+      for (int i = 0; i < 4; ++i) p[i] = __floats2bfloat162_rn(xn[2 * i], xn[2 * i + 1]);
+      *reinterpret_cast<int4*>(act + tc16_offset(gt, 0)) = *reinterpret_cast<int4*>(p);
+      *reinterpret_cast<int4*>(act + tc16_offset(gt, 8)) = make_int4(0, 0, 0, 0);
     }
-    // layer 2 (tensor cores)
-    ok = group_gemm(act, w2, tmem, mb, parity, g, gt);
+    ok = group_layer(1, act, w1t, tmem, mb, parity, g, gt);
     if (!ok) break;
     for (int c = 0; c < 4; ++c) {
       float v[32];
       tmem_ld32(taddr + c * 32, v);
 #pragma unroll
-      for (int i = 0; i < 32; ++i) v[i] = gelu_fast(v[i] + b2[c * 32 + i]);
+      for (int i = 0; i < 32; ++i) v[i] = gelu_fast5(v[i] + b1[c * 32 + i]);
 #pragma unroll
       for (int q = 0; q < 4; ++q) store8(act, gt, c * 4 + q, v + q * 8);
     }
-    // layer 3 (tensor cores) and layer 4 (FP32 pipes), fused in the read-back
-    ok = group_gemm(act, w3, tmem, mb, parity, g, gt);
+    // layer 2
+    ok = group_layer(2, act, w2, tmem, mb, parity, g, gt);
     if (!ok) break;
-    float y[OUT];
-#pragma unroll
-    for (int j = 0; j < OUT; ++j) y[j] = b4[j];
     for (int c = 0; c < 4; ++c) {
       float v[32];
       tmem_ld32(taddr + c * 32, v);
 #pragma unroll
-      for (int i = 0; i < 32; ++i) {
-        const float h = bf16r(gelu_fast(v[i] + b3[c * 32 + i]));
+      for (int i = 0; i < 32; ++i) v[i] = gelu_fast5(v[i] + b2[c * 32 + i]);
 #pragma unroll
-        for (int j = 0; j < OUT; ++j) y[j] = fmaf(w4[j * H + c * 32 + i], h, y[j]);
-      }
+      for (int q = 0; q < 4; ++q) store8(act, gt, c * 4 + q, v + q * 8);
     }
+    // layer 3
+    ok = group_layer(2, act, w3, tmem, mb, parity, g, gt);
+    if (!ok) break;
+    for (int c = 0; c < 4; ++c) {
+      float v[32];
+      tmem_ld32(taddr + c * 32, v);
+#pragma unroll
+      for (int i = 0; i < 32; ++i) v[i] = gelu_fast5(v[i] + b3[c * 32 + i]);
+#pragma unroll
+      for (int q = 0; q < 4; ++q) store8(act, gt, c * 4 + q, v + q * 8);
+    }
+    // layer 4 (tensor cores, N = 5 padded to 16)
+    ok = group_layer(4, act, w4t, tmem, mb, parity, g, gt);
+    if (!ok) break;
+    float y[16];
+    tmem_ld16(taddr, y);
     if (valid) {
 #pragma unroll
       for (int j = 0; j < OUT; ++j) {
-        float o = fmaf(y[j], nrm[13 + j], nrm[8 + j]);
+        float o = fmaf(y[j] + b4[j], nrm[13 + j], nrm[8 + j]);
         if (physical) {
           if (j == 0) o = expf(o + lnN);
           else if (j == 1) o = 1.f / (1.f + expf(-o));
@@ -608,7 +678,14 @@ __global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float*
 // BF16 tensor-core copies and BF16-rounded narrow layers from the masters.
 __global__ void prepare_kernel(const float* __restrict__ p, float* __restrict__ w1r, float* __restrict__ w4r,
                                __nv_bfloat16* __restrict__ w2tc, __nv_bfloat16* __restrict__ w3tc,
-                               __nv_bfloat16* __restrict__ w2ttc, __nv_bfloat16* __restrict__ w3ttc) {
+                               __nv_bfloat16* __restrict__ w2ttc, __nv_bfloat16* __restrict__ w3ttc,
+                               __nv_bfloat16* __restrict__ w1tc, __nv_bfloat16* __restrict__ w4tc) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < H * 16; i += gridDim.x * blockDim.x) {
+    const int o = i / 16, k = i % 16;  // layer 1: rows = out (128), K = in (4 of 16)
+    w1tc[tc16_offset(o, k)] = __float2bfloat16_rn(k < IN ? p[OFF_W1 + o * IN + k] : 0.f);
+    const int r = i / H, kk = i % H;   // layer 4: rows = out (5 of 16), K = in (128)
+    w4tc[tc_offset(r, kk)] = __float2bfloat16_rn(r < OUT ? p[OFF_W4 + r * H + kk] : 0.f);
+  }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < H * H; i += gridDim.x * blockDim.x) {
     const int o = i / H, k = i % H;
     w2tc[tc_offset(o, k)] = __float2bfloat16_rn(p[OFF_W2 + i]);   // B of h W2^T: rows = out, K = in
@@ -765,7 +842,7 @@ __global__ void gamma_fit_kernel(const double* __restrict__ hist, int64_t n, int
   }
 }
 
-constexpr size_t kInferSmem = (2 + kGroups) * TILE_BYTES + (H * IN + 3 * H + OUT * H + 8 + 24) * 4 + 8 * kGroups + 16;
+constexpr size_t kInferSmem = (2 + kGroups) * TILE_BYTES + 2 * H * 16 * 2 + (3 * H + 8 + 24) * 4 + 8 * kGroups + 16;
 constexpr size_t kTrainSmem = 3 * TILE_BYTES + (H * IN + OUT * H + 8 + TILE * OUT + 8) * 4 + 16 + 16;
 constexpr size_t kTestSmem = 2 * TILE_BYTES + 32;
 
@@ -814,6 +891,8 @@ mlp::DevParams dev_params(pp_mlp* m) {
   P.w2tc = m->d_tc;
   P.w3tc = m->d_tc + mlp::TILE * mlp::H;
   P.w2ttc = m->d_tc + 2 * mlp::TILE * mlp::H;
+  P.w1tc = m->d_tc + 4 * mlp::TILE * mlp::H;
+  P.w4tc = m->d_tc + 4 * mlp::TILE * mlp::H + mlp::H * 16;
   P.w3ttc = m->d_tc + 3 * mlp::TILE * mlp::H;
   P.norm = m->d_norm;
   P.error = m->d_error;
@@ -822,7 +901,8 @@ mlp::DevParams dev_params(pp_mlp* m) {
 
 cudaError_t prepare(pp_mlp* m, cudaStream_t s) {
   mlp::prepare_kernel<<<64, 256, 0, s>>>(m->d_params, m->d_w1r, m->d_w4r, m->d_tc, m->d_tc + mlp::TILE * mlp::H,
-                                         m->d_tc + 2 * mlp::TILE * mlp::H, m->d_tc + 3 * mlp::TILE * mlp::H);
+                                         m->d_tc + 2 * mlp::TILE * mlp::H, m->d_tc + 3 * mlp::TILE * mlp::H,
+                                         m->d_tc + 4 * mlp::TILE * mlp::H, m->d_tc + 4 * mlp::TILE * mlp::H + mlp::H * 16);
   pp::count_launches(1);
   return cudaGetLastError();
 }
@@ -853,7 +933,7 @@ pp_status pp_mlp_create(int device, uint64_t seed, pp_mlp** out) {
   if ((e = cudaMalloc(&m->d_params, mlp::N_PARAMS * 4)) || (e = cudaMalloc(&m->d_grad, mlp::N_PARAMS * 4)) ||
       (e = cudaMalloc(&m->d_m, mlp::N_PARAMS * 4)) || (e = cudaMalloc(&m->d_v, mlp::N_PARAMS * 4)) ||
       (e = cudaMalloc(&m->d_w1r, mlp::H * mlp::IN * 4)) || (e = cudaMalloc(&m->d_w4r, mlp::OUT * mlp::H * 4)) ||
-      (e = cudaMalloc(&m->d_tc, 4 * mlp::TILE_BYTES)) || (e = cudaMalloc(&m->d_norm, 32 * 4)) ||
+      (e = cudaMalloc(&m->d_tc, 4 * mlp::TILE_BYTES + 2 * mlp::H * 16 * 2)) || (e = cudaMalloc(&m->d_norm, 32 * 4)) ||
       (e = cudaMalloc(&m->d_error, 16)) || (e = cudaMalloc(&m->d_loss, 16))) {
     cudaGetLastError();
     for (void* b : {(void*)m->d_params, (void*)m->d_grad, (void*)m->d_m, (void*)m->d_v, (void*)m->d_w1r,

@@ -34,14 +34,6 @@ def test_device_philox_and_uniform_bit_exact(propagator):
     for i in range(256):
         want = O.philox4x32_10([int(x) for x in ctr[i, :4]], [int(x) for x in ctr[i, 4:]])
         assert [int(x) for x in out[i]] == want
-    # the kernels' form: rounds 1-2 from per-pair / per-photon constants, the library key
-    ctr4 = rng.integers(0, 2**32, size=(512, 4), dtype=np.uint64)
-    ctr4[0] = 0
-    ctr4[1] = 0xFFFFFFFF
-    out = propagator.device_eval(12, ctr4.astype(np.float64))
-    key = [0x243F6A88, 0x85A308D3]
-    for i in range(len(ctr4)):
-        assert [int(x) for x in out[i]] == O.philox4x32_10([int(x) for x in ctr4[i]], key)
     w = rng.integers(0, 2**32, size=1000, dtype=np.uint64)
     u = propagator.device_eval(1, w.astype(np.float64))[:, 0]
     np.testing.assert_array_equal(u, [O.uniform(int(x)) for x in w])
