@@ -1071,10 +1071,12 @@ def run_ours(args):
                        "what": "device time of one 4096-pair batch solve"},
         "roofline": {"bound": "mufu", "achieved": a_mufu / 1e9, "peak": peaks["mufu_ops"] / 1e9,
                      "unit": "Gop/s", "frac": f_mufu,
-                     "traffic": roofline.NCU_DRAM_BYTES_PER_PHOTON * photons_local[0],
-                     "traffic_note": "DRAM bytes per launch: ncu capture of a 2.5e8-photon launch scaled by photons",
+                     "traffic": roofline.NCU_DRAM_BYTES_PER_LAUNCH,
+                     "traffic_note": "dram__bytes_read.sum + dram__bytes_write.sum of a full-size launch of this "
+                                     "workload (ncu, one pass, mean of two timed launches after an L2 flush); the "
+                                     "histograms and hits accumulate in L2 and reach DRAM after the launch",
                      "issue_active_ncu": roofline.NCU_ISSUE_ACTIVE,
-                     "branch_efficiency_ncu": roofline.NCU_BRANCH_UNIFORM,
+                     "lanes_active_ncu": roofline.NCU_LANES_ACTIVE,
                      "note": "issue-bound: ncu shows {:.0%} of issue slots busy (ALU pipe {:.0%}, FMA {:.0%}, XU {:.0%})".format(
                          roofline.NCU_ISSUE_ACTIVE, roofline.NCU_PIPES["alu"], roofline.NCU_PIPES["fma"],
                          roofline.NCU_PIPES["xu"]),

@@ -41,13 +41,15 @@ def op_counts(steps, photons_iso, photons_cone, algorithmic=False):
     return mufu, fp32, blocks
 
 
-# DRAM traffic of the batched kernel per photon, measured with ncu
-# (dram__bytes_read.sum + dram__bytes_write.sum) on one launch of 2.524e8
-# photons (512 mixed pairs, <= 1e6 photons each): 117.8 KB read, 0 B written.
-# Hit records and FP64 histogram reductions stay in L2 during a launch, so
-# the traffic grows with the photon count; bench.py scales it to its launch.
-NCU_DRAM_BYTES_PER_PHOTON = 117.76e3 / 252387747
-# Issue slots busy in the same capture (smsp__issue_active).
-NCU_ISSUE_ACTIVE = 0.775
-NCU_PIPES = {"alu": 0.503, "fma": 0.338, "xu": 0.284}  # pipe utilisation, same capture
-NCU_BRANCH_UNIFORM = 0.914  # smsp__sass_average_branch_targets_threads_uniform, same capture
+# ncu figures of the batched kernel as shipped.
+# DRAM traffic of one launch of the 4096-pair benchmark batch (5.75e9
+# photons), full size, `--metrics dram__bytes_read.sum,dram__bytes_write.sum
+# --cache-control none` (one pass): the two timed launches after an L2 flush
+# read 2.4 and 3.4 MB and wrote 25.5 and 34.7 MB.  The rest of a step's
+# algorithmic bytes (zeroed and accumulated FP64 histograms, hit records)
+# stays in the 126 MB L2 during the launch and reaches DRAM afterwards.
+NCU_DRAM_BYTES_PER_LAUNCH = 0.5 * ((2.43 + 25.48) + (3.35 + 34.66)) * 1e6
+# Issue and pipes on one launch of 512 mixed pairs (<= 1e6 photons each).
+NCU_ISSUE_ACTIVE = 0.778
+NCU_PIPES = {"alu": 0.487, "fma": 0.347, "xu": 0.322}  # pipe utilisation, same capture
+NCU_LANES_ACTIVE = 30.0  # threads per executed warp instruction, same capture

@@ -50,6 +50,7 @@ class Server:
         self._h = h
         self.bins = cfg.opts.hist_bins
         self._npairs = {}
+        self._hitbuf = None  # reused by result(): one allocation, not one per request
 
     def close(self):
         if getattr(self, "_h", None):
@@ -75,7 +76,9 @@ class Server:
     def result(self, rid: int, timeout_s: float = 60.0, hit_capacity: int = 1 << 20) -> RequestResult:
         self.wait(rid, timeout_s)
         n, _ = self._npairs.pop(rid)
-        hits = np.zeros(hit_capacity, dtype=_lib.HIT32_DTYPE)
+        if self._hitbuf is None or len(self._hitbuf) < hit_capacity:
+            self._hitbuf = np.empty(hit_capacity, dtype=_lib.HIT32_DTYPE)
+        hits = self._hitbuf
         stats = np.zeros((n, _lib.N_STATS))
         hist = np.zeros((n, max(self.bins, 1)))
         nh = ctypes.c_int64()
@@ -119,9 +122,12 @@ def _percentiles(lat):
 
 def run_open_loop(server: Server, arrivals, reqs, timeout_s=120.0):
     """Submits each request at its arrival time (open loop) from this thread and
-    collects results on a second thread.  Latency = completion - arrival."""
+    collects results on a second thread.  Latency = completion - scheduled
+    arrival: the server's submit-to-completion time plus any delay of the
+    submission behind its scheduled arrival."""
     ids = [None] * len(reqs)
     results = [None] * len(reqs)
+    late = [0.0] * len(reqs)
     submitted = threading.Semaphore(0)
 
     def collect():
@@ -136,14 +142,16 @@ def run_open_loop(server: Server, arrivals, reqs, timeout_s=120.0):
         dt = t0 + t - time.perf_counter()
         if dt > 0:
             time.sleep(dt)
+        late[i] = max(0.0, time.perf_counter() - (t0 + t))
         ids[i] = server.submit(r)
         submitted.release()
     th.join()
     wall = time.perf_counter() - t0
     photons = float(sum(int(r["n_photons"].sum()) for r in reqs))
-    lat = [x.latency_s for x in results]
+    lat = [x.latency_s + d for x, d in zip(results, late)]
     out = {"requests": len(reqs), "photons": photons, "wall_s": wall, "photons_per_s": photons / wall,
-           "overflow_requests": int(sum(x.overflow for x in results))}
+           "overflow_requests": int(sum(x.overflow for x in results)),
+           "max_submit_delay_ms": float(max(late) * 1e3) if late else 0.0}
     out.update(_percentiles(lat))
     return out, results
 
