@@ -5,7 +5,11 @@
 // slot is free, packs them into one batch (one pair list, one launch of the
 // batched kernel with the slot's own work-queue scratch) on the slot's
 // stream, copies the results back on that stream and enqueues a host
-// function that marks the slot finished.  Up to max_inflight slots run at
+// function that marks the slot finished.  A batch takes requests only while
+// their reserved hits fit the slot's hit buffers (sized at creation), so a
+// running server does not reallocate: a device free synchronises the device
+// and pinning pages takes milliseconds, both under the server lock that
+// submit() also takes.  Up to max_inflight slots run at
 // once, so a request that arrives while batches are on the device is admitted
 // as soon as a slot and memory free up, and its batch overlaps the running
 // ones.  The host function only sets an atomic flag and notifies; it takes no
@@ -217,10 +221,15 @@ bool launch_slot(pp_server* S, Slot& s) {
   pp::Range range_("pp_server batch launch");
   std::vector<ReqPtr> take;
   int64_t pairs = 0, cap = 0, reserve = 0;
+  // the slot's hit buffer as it is: a batch that would outgrow it waits for the
+  // next slot, so that a running server does not reallocate (a free
+  // synchronises the device, and pinning pages takes milliseconds)
+  const int64_t have_hits = (int64_t)(std::min(s.d_hits.bytes, s.h_hits.bytes) / sizeof(pp_hit32));
   while (!S->waiting.empty()) {
     const ReqPtr& r = S->waiting.front();
     const int64_t n = (int64_t)r->pairs.size();
     if (!take.empty() && pairs + n > S->cfg.max_pairs_per_batch) break;
+    if (!take.empty() && cap + r->hit_cap > have_hits) break;
     if (S->reserved + reserve + r->reserve > S->cfg.hbm_budget_bytes) break;  // wait for memory
     take.push_back(r);
     pairs += n;
@@ -356,7 +365,7 @@ pp_status pp_server_create(pp_ctx* ctx, const pp_server_config* cfg, pp_server**
     if (s->d_pairs.ensure(np * sizeof(pp_pair)) || s->d_offsets.ensure((np + 1) * 8) || s->d_queue.ensure(64) ||
         s->d_counters.ensure(64) || s->d_stats.ensure(np * PP_STATS * 8) || s->d_hist.ensure(np * bins * 8) ||
         s->h_pairs.ensure(np * sizeof(pp_pair)) || s->h_counters.ensure(64) || s->h_stats.ensure(np * PP_STATS * 8) ||
-        s->h_hist.ensure(np * bins * 8) || s->d_hits.ensure((size_t)16 << 20) || s->h_hits.ensure((size_t)16 << 20))
+        s->h_hist.ensure(np * bins * 8) || s->d_hits.ensure((size_t)64 << 20) || s->h_hits.ensure((size_t)64 << 20))
       cudaGetLastError();  // a failed pre-allocation is retried at launch
     S->slots.push_back(std::move(s));
   }
