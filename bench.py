@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--overload-seconds", type=float, default=10.0,
                     help="length of the overload serving sample (0 = skip)")
     ap.add_argument("--workload", choices=["batch", "serving", "surrogate", "surrogate-infer", "cone-grid", "point",
-                                           "fits", "event", "llh"], default="batch")
+                                           "fits", "event", "llh", "large-pairs"], default="batch")
     ap.add_argument("--fit-photons", type=int, default=100_000_000, help="fits workload: photons per distance")
     ap.add_argument("--fit-distances", type=int, default=250)
     ap.add_argument("--fit-angles", type=int, default=250)
@@ -438,6 +438,33 @@ def run_cone_grid(args):
             "hits_per_pair": rp.stats[:, 0].tolist(), "sum_w_per_pair": rp.stats[:, 1].tolist(),
             "identical_stats": bool(np.allclose(rp.stats, rb.stats, rtol=1e-9))}
     print(json.dumps(line), flush=True)
+
+
+def run_large_pairs(args):
+    """--workload large-pairs: eight pairs of 9e6-1e7 photons (the decade that
+    holds 90 % of the benchmark batch's photons), 20-40 m, one launch per
+    pair and one batched launch, host API, twice; photons/s of each."""
+    import torch
+    import photonprop_b200 as pp
+    torch.cuda.set_device(0)
+    medium = pp.make_seawater(35.0, 2.0)
+    spec = pp.CherenkovSpectrum((300.0, 800.0), 20, medium)
+    b = pp.batches.mixed_batch(8, seed=77, n_min=9e6, n_max=1e7, d_min=20.0, d_max=40.0)
+    ro = pp.RunOptions(**RUN_KW)
+    with pp.Propagator(medium, spec, pp.p_one_pmt_acc, device=0) as prop:
+        tp = tb = 0.0
+        for _ in range(2):
+            t0 = time.perf_counter()
+            a = prop.propagate_plain(b, ro)
+            tp = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            c = prop.propagate(b, ro)
+            tb = time.perf_counter() - t0
+    photons = float(b["n_photons"].sum())
+    print(json.dumps({"metric": "photons/s on eight 9e6-1e7-photon pairs, plain vs batched (host API)",
+                      "unit": UNIT, "plain_photons_per_s": photons / tp, "batched_photons_per_s": photons / tb,
+                      "hits_plain": a.n_hits, "hits_batched": c.n_hits, "n_gpus": 1, "data": "synthetic"}),
+          flush=True)
 
 
 def run_point(args):
@@ -1144,6 +1171,8 @@ def main():
         run_event(args)
     elif args.workload == "llh":
         run_llh(args)
+    elif args.workload == "large-pairs":
+        run_large_pairs(args)
     elif args.workload == "surrogate-infer":
         import torch
         torch.cuda.set_device(0)
