@@ -359,16 +359,30 @@ __global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, co
   uint32_t parity = 0;
   bool ok = true;
 
-  for (int64_t tile = (int64_t)blockIdx.x * kGroups + g; ok && tile * TILE < n; tile += (int64_t)gridDim.x * kGroups) {
+  const int64_t tile_step = (int64_t)gridDim.x * kGroups;
+  // the row's features, loaded one tile ahead so that the global loads
+  // overlap the previous tile's layers
+  float xr[IN];
+  {
+    const int64_t row0 = ((int64_t)blockIdx.x * kGroups + g) * TILE + gt;
+#pragma unroll
+    for (int j = 0; j < IN; ++j) xr[j] = row0 < n ? x[row0 * IN + j] : nrm[j];
+  }
+  for (int64_t tile = (int64_t)blockIdx.x * kGroups + g; ok && tile * TILE < n; tile += tile_step) {
     const int64_t row = tile * TILE + gt;
     const bool valid = row < n;
     float xn[8];
     float lnN = 0.f;
 #pragma unroll
     for (int j = 0; j < IN; ++j) {
-      const float raw = valid ? x[row * IN + j] : nrm[j];
+      const float raw = xr[j];
       if (j == 2) lnN = raw * 2.302585092994046f;
       xn[j] = (raw - nrm[j]) / nrm[4 + j];
+    }
+    {
+      const int64_t nrow = row + tile_step * TILE;
+#pragma unroll
+      for (int j = 0; j < IN; ++j) xr[j] = nrow < n ? x[nrow * IN + j] : nrm[j];
     }
 #pragma unroll
     for (int j = IN; j < 8; ++j) xn[j] = 0.f;
