@@ -52,6 +52,39 @@ def test_forward_matches_oracle():
     net.close()
 
 
+@pytest.mark.parametrize("n", [1000, 100_000])
+def test_forward_with_biases_and_normalization_matches_oracle(n):
+    """Non-zero biases in every layer and a non-trivial feature / output
+    normalisation (a fresh network has zero biases and the tests above use
+    the identity normalisation)."""
+    import torch
+    net = sg.MLP(0, 7)
+    rng = np.random.default_rng(n)
+    p = net.get_params().astype(np.float64)
+    off = 0
+    for name, shape in omlp.SIZES:
+        k = int(np.prod(shape))
+        if name.startswith("b"):
+            p[off:off + k] = rng.normal(scale=0.5, size=k)
+        off += k
+    net.set_params(p.astype(np.float32))
+    p = net.get_params().astype(np.float64)
+    xm, xs = rng.normal(size=4).astype(np.float32), rng.uniform(0.5, 2.0, 4).astype(np.float32)
+    ym, ys = rng.normal(size=5).astype(np.float32), rng.uniform(0.5, 2.0, 5).astype(np.float32)
+    net.set_normalization(xm, xs, ym, ys)
+    x = (xm + xs * rng.normal(size=(n, 4))).astype(np.float32)
+    d_x = torch.from_numpy(x).cuda()
+    d_o = torch.empty((5, n), dtype=torch.float32, device="cuda")
+    net.forward(d_x, d_o, n, physical=False)
+    y = d_o.cpu().numpy().T
+    ref, _ = omlp.forward(p, ((x - xm) / xs).astype(np.float64))  # standardised as the kernel does, in FP32
+    ref = ref * ys + ym
+    err = np.abs(y - ref) / (1 + np.abs(ref))
+    print("max scaled error", err.max())
+    assert err.max() <= 2e-2, err.max()
+    net.close()
+
+
 def test_gradients_match_oracle():
     import torch
     net = _net_with_norm(seed=3)
