@@ -53,21 +53,16 @@ __device__ __forceinline__ float gelu(float z) {
   const float u = 0.7978845608028654f * fmaf(0.044715f * z, z * z, z);
   return 0.5f * z * (1.f + tanhf(u));
 }
-// Inference GELU with the MUFU tanh (tanh.approx.f32, relative error below
-// 2^-10, under the BF16 rounding that follows it), in five FP32 operations:
-// u = z (k + k c z^2), GELU = z (1/2 + t/2).
-__device__ __forceinline__ float gelu_fast5(float z) {
+// Twice the inference GELU with the MUFU tanh (tanh.approx.f32, relative
+// error below 2^-10, under the BF16 rounding that follows it), in four FP32
+// operations: u = z (k + k c z^2), 2 GELU = z (1 + t).  The factor 1/2 is
+// folded into the next layer's weights (exact: a power of two commutes with
+// the BF16 rounding of both the weights and the activations).
+__device__ __forceinline__ float gelu2_fast(float z) {
   const float u = z * fmaf(0.7978845608028654f * 0.044715f, z * z, 0.7978845608028654f);
   float t;
   asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-  return z * fmaf(0.5f, t, 0.5f);
-}
-__device__ __forceinline__ float gelu_fast(float z) {
-  const float u = 0.7978845608028654f * fmaf(0.044715f * z, z * z, z);
-  float t;
-  asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(u));
-  const float hz = 0.5f * z;
-  return fmaf(hz, t, hz);
+  return fmaf(z, t, z);
 }
 __device__ __forceinline__ float gelu_grad(float z) {
   const float u = 0.7978845608028654f * fmaf(0.044715f * z, z * z, z);
@@ -220,7 +215,9 @@ struct DevParams {
   const __nv_bfloat16* w2tc;   // W2 as the B operand of h W2^T (canonical tile)
   const __nv_bfloat16* w3tc;
   const __nv_bfloat16* w1tc;   // W1 as the B operand of x W1^T: 128 rows x K 16 (4 used)
-  const __nv_bfloat16* w4tc;   // W4 as the B operand of h W4^T: 16 rows (5 used) x K 128
+  const __nv_bfloat16* w4tc;   // W4 / 2 as the B operand of h W4^T: 16 rows (5 used) x K 128
+  const __nv_bfloat16* w2h;    // W2 / 2, W3 / 2: inference B operands (they take 2 GELU)
+  const __nv_bfloat16* w3h;
   const __nv_bfloat16* w2ttc;  // W2^T as the B operand of dz W2
   const __nv_bfloat16* w3ttc;
   const float* norm;     // x_mean[4], x_std[4], y_mean[5], y_std[5]
@@ -244,8 +241,11 @@ __device__ __forceinline__ void load_tile(__nv_bfloat16* dst, const __nv_bfloat1
 // of layers 2 and 3 in shared memory; each owns an activation tile, an
 // mbarrier and 128 of the CTA's TMEM columns, and walks its own sequence of
 // row tiles with group-local named barriers.  While one group's MMAs run on
-// the tensor cores the others run their bias/GELU epilogues on the FP32 and
-// MUFU pipes, and sixteen warps per SM keep those pipes busy.
+// the tensor cores the others run their GELU epilogues on the FP32 and MUFU
+// pipes, and sixteen warps per SM keep those pipes busy.  The biases of the
+// hidden layers are added by the tensor cores and the GELU's factor 1/2 sits
+// in the next layer's weights, so an activation costs four FP32 operations,
+// one tanh and half a BF16 pack.
 constexpr int kGroups = 4, INFER_THREADS = kGroups * THREADS;
 
 __device__ __forceinline__ void group_sync(int g) {
@@ -285,10 +285,16 @@ __device__ __forceinline__ bool group_gemm(const __nv_bfloat16* a, const __nv_bf
   return ok;
 }
 
-// The group's MMAs of one layer; kind 1: x (128 x 16) W1^T, one MMA;
-// kind 2: h (128 x 128) W^T, eight MMAs; kind 4: h W4^T with N = 16.
+// The group's MMAs of one layer; kind 1: x (128 x 16) W1^T, one MMA (the
+// bias rides in K columns 4 and 5: x has ones there, W1 the bias split into
+// BF16 hi and lo); kind 2: h (128 x 128) W^T, eight MMAs, then a ninth,
+// ones (128 x 16) times the bias tile, that adds the bias in the
+// accumulator; kind 4: h W4^T with N = 16.  The epilogues then read z with
+// its bias and spend no FP32 add on it.
 __device__ __forceinline__ bool group_layer(int kind, const __nv_bfloat16* a, const __nv_bfloat16* b, uint32_t tmem,
-                                            uint32_t mbar, uint32_t& parity, int g, int gt) {
+                                            uint32_t mbar, uint32_t& parity, int g, int gt,
+                                            const __nv_bfloat16* ones = nullptr,
+                                            const __nv_bfloat16* bias = nullptr) {
   fence_async_smem();
   tc_fence_before();
   group_sync(g);
@@ -302,6 +308,8 @@ __device__ __forceinline__ bool group_layer(int kind, const __nv_bfloat16* a, co
 #pragma unroll
       for (int k = 0; k < 8; ++k)
         mma_idesc(tmem, smem_desc(sa + k * 256, 128, 2048), smem_desc(sb + k * 256, 128, 2048), idesc, k > 0);
+      if (kind == 2)  // + 1 (bias hi, bias lo): the layer's bias, one more K = 16 step
+        mma_idesc(tmem, smem_desc(smem_u32(ones), 128, 256), smem_desc(smem_u32(bias), 128, 256), kIdesc, 1u);
     }
     mma_commit(mbar);
   }
@@ -316,30 +324,31 @@ __global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, co
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   __nv_bfloat16* w2 = reinterpret_cast<__nv_bfloat16*>(smem_raw);
   __nv_bfloat16* w3 = w2 + TILE * H;
-  __nv_bfloat16* w1t = w3 + TILE * H;   // 128 x 16
+  __nv_bfloat16* w1t = w3 + TILE * H;   // 128 x 16: W1 in K 0..3, b1 (hi, lo) in K 4, 5
   __nv_bfloat16* w4t = w1t + H * 16;    // 16 x 128
-  __nv_bfloat16* acts = w4t + 16 * H;   // kGroups activation tiles (the x tile is the first 4 KB of one)
-  float* b1 = reinterpret_cast<float*>(acts + kGroups * TILE * H);
-  float* b2 = b1 + H;
-  float* b3 = b2 + H;
-  float* b4 = b3 + H;
+  __nv_bfloat16* b2t = w4t + 16 * H;    // 128 x 16: b2 (hi, lo) in K 0, 1
+  __nv_bfloat16* b3t = b2t + H * 16;
+  __nv_bfloat16* ones = b3t + H * 16;   // 128 x 16: 1 in K 0, 1
+  __nv_bfloat16* acts = ones + TILE * 16;  // kGroups activation tiles (the x tile is the first 4 KB of one)
+  float* b4 = reinterpret_cast<float*>(acts + kGroups * TILE * H);
   float* nrm = b4 + 8;
   uint64_t* mbars = reinterpret_cast<uint64_t*>(nrm + 24);
   uint32_t* tslot = reinterpret_cast<uint32_t*>(mbars + kGroups);
 
   const int t = threadIdx.x;
   const int g = t >> 7, gt = t & (THREADS - 1);  // group, thread (= row) within the group
-  load_tile(w2, P.w2tc);
-  load_tile(w3, P.w3tc);
+  load_tile(w2, P.w2h);
+  load_tile(w3, P.w3h);
   {
     const int4* s1 = reinterpret_cast<const int4*>(P.w1tc);
     int4* d1 = reinterpret_cast<int4*>(w1t);
-    for (int i = t; i < 2 * H * 16 * 2 / 16; i += INFER_THREADS) d1[i] = s1[i];  // both 4 KB tiles
+    for (int i = t; i < 4 * H * 16 * 2 / 16; i += INFER_THREADS) d1[i] = s1[i];  // W1, W4, b2, b3 tiles
   }
-  for (int i = t; i < H; i += INFER_THREADS) {
-    b1[i] = P.p[OFF_B1 + i];
-    b2[i] = P.p[OFF_B2 + i];
-    b3[i] = P.p[OFF_B3 + i];
+  for (int i = t; i < TILE * 16 / 8; i += INFER_THREADS) {  // the ones tile, 8 columns per 16-byte word
+    const int row = i >> 1, k8 = i & 1;
+    const uint32_t one2 = 0x3F803F80u;  // two BF16 ones
+    *reinterpret_cast<int4*>(ones + tc16_offset(row, k8 * 8)) =
+        k8 == 0 ? make_int4((int)one2, 0, 0, 0) : make_int4(0, 0, 0, 0);
   }
   if (t < OUT) b4[t] = P.p[OFF_B4 + t];
   if (t < 18) nrm[t] = P.norm[t];
@@ -384,8 +393,10 @@ __global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, co
 #pragma unroll
       for (int j = 0; j < IN; ++j) xr[j] = nrow < n ? x[nrow * IN + j] : nrm[j];
     }
+    xn[IN] = 1.f;  // times the bias columns of W1
+    xn[IN + 1] = 1.f;
 #pragma unroll
-    for (int j = IN; j < 8; ++j) xn[j] = 0.f;
+    for (int j = IN + 2; j < 8; ++j) xn[j] = 0.f;
     // layer 1 (tensor cores, K = 4 padded to 16): the row's x in the x tile
     {
       __align__(16) __nv_bfloat162 p[4];
@@ -400,29 +411,29 @@ __global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, co
       float v[32];
       tmem_ld32(taddr + c * 32, v);
 #pragma unroll
-      for (int i = 0; i < 32; ++i) v[i] = gelu_fast5(v[i] + b1[c * 32 + i]);
+      for (int i = 0; i < 32; ++i) v[i] = gelu2_fast(v[i]);
 #pragma unroll
       for (int q = 0; q < 4; ++q) store8(act, gt, c * 4 + q, v + q * 8);
     }
     // layer 2
-    ok = group_layer(2, act, w2, tmem, mb, parity, g, gt);
+    ok = group_layer(2, act, w2, tmem, mb, parity, g, gt, ones, b2t);
     if (!ok) break;
     for (int c = 0; c < 4; ++c) {
       float v[32];
       tmem_ld32(taddr + c * 32, v);
 #pragma unroll
-      for (int i = 0; i < 32; ++i) v[i] = gelu_fast5(v[i] + b2[c * 32 + i]);
+      for (int i = 0; i < 32; ++i) v[i] = gelu2_fast(v[i]);
 #pragma unroll
       for (int q = 0; q < 4; ++q) store8(act, gt, c * 4 + q, v + q * 8);
     }
     // layer 3
-    ok = group_layer(2, act, w3, tmem, mb, parity, g, gt);
+    ok = group_layer(2, act, w3, tmem, mb, parity, g, gt, ones, b3t);
     if (!ok) break;
     for (int c = 0; c < 4; ++c) {
       float v[32];
       tmem_ld32(taddr + c * 32, v);
 #pragma unroll
-      for (int i = 0; i < 32; ++i) v[i] = gelu_fast5(v[i] + b3[c * 32 + i]);
+      for (int i = 0; i < 32; ++i) v[i] = gelu2_fast(v[i]);
 #pragma unroll
       for (int q = 0; q < 4; ++q) store8(act, gt, c * 4 + q, v + q * 8);
     }
@@ -693,12 +704,22 @@ __global__ void adam_kernel(float* __restrict__ p, float* __restrict__ g, float*
 __global__ void prepare_kernel(const float* __restrict__ p, float* __restrict__ w1r, float* __restrict__ w4r,
                                __nv_bfloat16* __restrict__ w2tc, __nv_bfloat16* __restrict__ w3tc,
                                __nv_bfloat16* __restrict__ w2ttc, __nv_bfloat16* __restrict__ w3ttc,
-                               __nv_bfloat16* __restrict__ w1tc, __nv_bfloat16* __restrict__ w4tc) {
+                               __nv_bfloat16* __restrict__ w1tc, __nv_bfloat16* __restrict__ w4tc,
+                               __nv_bfloat16* __restrict__ b2t, __nv_bfloat16* __restrict__ b3t,
+                               __nv_bfloat16* __restrict__ w2h, __nv_bfloat16* __restrict__ w3h) {
+  // a bias as two BF16 columns, hi + lo = b to about 2^-16 relative
+  auto split = [](float b, int part) {
+    const __nv_bfloat16 hi = __float2bfloat16_rn(b);
+    return part == 0 ? hi : __float2bfloat16_rn(b - __bfloat162float(hi));
+  };
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < H * 16; i += gridDim.x * blockDim.x) {
-    const int o = i / 16, k = i % 16;  // layer 1: rows = out (128), K = in (4 of 16)
-    w1tc[tc16_offset(o, k)] = __float2bfloat16_rn(k < IN ? p[OFF_W1 + o * IN + k] : 0.f);
-    const int r = i / H, kk = i % H;   // layer 4: rows = out (5 of 16), K = in (128)
-    w4tc[tc_offset(r, kk)] = __float2bfloat16_rn(r < OUT ? p[OFF_W4 + r * H + kk] : 0.f);
+    const int o = i / 16, k = i % 16;  // layer 1: rows = out (128), K = in (4 of 16), then b1 hi, lo
+    w1tc[tc16_offset(o, k)] = k < IN ? __float2bfloat16_rn(p[OFF_W1 + o * IN + k])
+                              : k < IN + 2 ? split(p[OFF_B1 + o], k - IN) : __float2bfloat16_rn(0.f);
+    b2t[tc16_offset(o, k)] = k < 2 ? split(p[OFF_B2 + o], k) : __float2bfloat16_rn(0.f);
+    b3t[tc16_offset(o, k)] = k < 2 ? split(p[OFF_B3 + o], k) : __float2bfloat16_rn(0.f);
+    const int r = i / H, kk = i % H;   // layer 4: rows = out (5 of 16), K = in (128); takes 2 GELU
+    w4tc[tc_offset(r, kk)] = __float2bfloat16_rn(r < OUT ? 0.5f * p[OFF_W4 + r * H + kk] : 0.f);
   }
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < H * H; i += gridDim.x * blockDim.x) {
     const int o = i / H, k = i % H;
@@ -706,6 +727,8 @@ __global__ void prepare_kernel(const float* __restrict__ p, float* __restrict__ 
     w3tc[tc_offset(o, k)] = __float2bfloat16_rn(p[OFF_W3 + i]);
     w2ttc[tc_offset(k, o)] = __float2bfloat16_rn(p[OFF_W2 + i]);  // B of dz W2: rows = in, K = out
     w3ttc[tc_offset(k, o)] = __float2bfloat16_rn(p[OFF_W3 + i]);
+    w2h[tc_offset(o, k)] = __float2bfloat16_rn(0.5f * p[OFF_W2 + i]);
+    w3h[tc_offset(o, k)] = __float2bfloat16_rn(0.5f * p[OFF_W3 + i]);
     if (i < H * IN) w1r[i] = bf16r(p[OFF_W1 + i]);
     if (i < OUT * H) w4r[i] = bf16r(p[OFF_W4 + i]);
   }
@@ -856,7 +879,7 @@ __global__ void gamma_fit_kernel(const double* __restrict__ hist, int64_t n, int
   }
 }
 
-constexpr size_t kInferSmem = (2 + kGroups) * TILE_BYTES + 2 * H * 16 * 2 + (3 * H + 8 + 24) * 4 + 8 * kGroups + 16;
+constexpr size_t kInferSmem = (2 + kGroups) * TILE_BYTES + 5 * H * 16 * 2 + (8 + 24) * 4 + 8 * kGroups + 16;
 constexpr size_t kTrainSmem = 3 * TILE_BYTES + (H * IN + OUT * H + 8 + TILE * OUT + 8) * 4 + 16 + 16;
 constexpr size_t kTestSmem = 2 * TILE_BYTES + 32;
 
@@ -874,7 +897,7 @@ struct pp_mlp {
   float* d_v = nullptr;
   float* d_w1r = nullptr;
   float* d_w4r = nullptr;
-  __nv_bfloat16* d_tc = nullptr;  // 4 tiles
+  __nv_bfloat16* d_tc = nullptr;  // 6 tiles of 128 x 128, then 4 of 128 x 16
   float* d_norm = nullptr;        // 18 (+ pad)
   int* d_error = nullptr;
   float* d_loss = nullptr;
@@ -905,8 +928,10 @@ mlp::DevParams dev_params(pp_mlp* m) {
   P.w2tc = m->d_tc;
   P.w3tc = m->d_tc + mlp::TILE * mlp::H;
   P.w2ttc = m->d_tc + 2 * mlp::TILE * mlp::H;
-  P.w1tc = m->d_tc + 4 * mlp::TILE * mlp::H;
-  P.w4tc = m->d_tc + 4 * mlp::TILE * mlp::H + mlp::H * 16;
+  P.w2h = m->d_tc + 4 * mlp::TILE * mlp::H;
+  P.w3h = m->d_tc + 5 * mlp::TILE * mlp::H;
+  P.w1tc = m->d_tc + 6 * mlp::TILE * mlp::H;
+  P.w4tc = P.w1tc + mlp::H * 16;
   P.w3ttc = m->d_tc + 3 * mlp::TILE * mlp::H;
   P.norm = m->d_norm;
   P.error = m->d_error;
@@ -914,9 +939,10 @@ mlp::DevParams dev_params(pp_mlp* m) {
 }
 
 cudaError_t prepare(pp_mlp* m, cudaStream_t s) {
-  mlp::prepare_kernel<<<64, 256, 0, s>>>(m->d_params, m->d_w1r, m->d_w4r, m->d_tc, m->d_tc + mlp::TILE * mlp::H,
-                                         m->d_tc + 2 * mlp::TILE * mlp::H, m->d_tc + 3 * mlp::TILE * mlp::H,
-                                         m->d_tc + 4 * mlp::TILE * mlp::H, m->d_tc + 4 * mlp::TILE * mlp::H + mlp::H * 16);
+  __nv_bfloat16* t = m->d_tc;
+  constexpr int T = mlp::TILE * mlp::H, S = mlp::H * 16;
+  mlp::prepare_kernel<<<64, 256, 0, s>>>(m->d_params, m->d_w1r, m->d_w4r, t, t + T, t + 2 * T, t + 3 * T, t + 6 * T,
+                                         t + 6 * T + S, t + 6 * T + 2 * S, t + 6 * T + 3 * S, t + 4 * T, t + 5 * T);
   pp::count_launches(1);
   return cudaGetLastError();
 }
@@ -947,7 +973,7 @@ pp_status pp_mlp_create(int device, uint64_t seed, pp_mlp** out) {
   if ((e = cudaMalloc(&m->d_params, mlp::N_PARAMS * 4)) || (e = cudaMalloc(&m->d_grad, mlp::N_PARAMS * 4)) ||
       (e = cudaMalloc(&m->d_m, mlp::N_PARAMS * 4)) || (e = cudaMalloc(&m->d_v, mlp::N_PARAMS * 4)) ||
       (e = cudaMalloc(&m->d_w1r, mlp::H * mlp::IN * 4)) || (e = cudaMalloc(&m->d_w4r, mlp::OUT * mlp::H * 4)) ||
-      (e = cudaMalloc(&m->d_tc, 4 * mlp::TILE_BYTES + 2 * mlp::H * 16 * 2)) || (e = cudaMalloc(&m->d_norm, 32 * 4)) ||
+      (e = cudaMalloc(&m->d_tc, 6 * mlp::TILE_BYTES + 4 * mlp::H * 16 * 2)) || (e = cudaMalloc(&m->d_norm, 32 * 4)) ||
       (e = cudaMalloc(&m->d_error, 16)) || (e = cudaMalloc(&m->d_loss, 16))) {
     cudaGetLastError();
     for (void* b : {(void*)m->d_params, (void*)m->d_grad, (void*)m->d_m, (void*)m->d_v, (void*)m->d_w1r,
