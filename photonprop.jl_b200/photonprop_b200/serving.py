@@ -51,6 +51,7 @@ class Server:
         self.bins = cfg.opts.hist_bins
         self._npairs = {}
         self._hitbuf = None  # reused by result(): one allocation, not one per request
+        self._hitbuf_lock = threading.Lock()  # result() may be called from several threads
 
     def close(self):
         if getattr(self, "_h", None):
@@ -76,19 +77,20 @@ class Server:
     def result(self, rid: int, timeout_s: float = 60.0, hit_capacity: int = 1 << 20) -> RequestResult:
         self.wait(rid, timeout_s)
         n, _ = self._npairs.pop(rid)
-        if self._hitbuf is None or len(self._hitbuf) < hit_capacity:
-            self._hitbuf = np.empty(hit_capacity, dtype=_lib.HIT32_DTYPE)
-        hits = self._hitbuf
         stats = np.zeros((n, _lib.N_STATS))
         hist = np.zeros((n, max(self.bins, 1)))
         nh = ctypes.c_int64()
         lat = ctypes.c_double()
-        st = self._L.pp_server_result(self._h, rid, hits.ctypes.data, hit_capacity, ctypes.byref(nh),
-                                      stats.ctypes.data, hist.ctypes.data, ctypes.byref(lat))
-        if st not in (_lib.PP_OK, _lib.PP_ERR_OVERFLOW):
-            _lib.check(st)
-        return RequestResult(hits[:min(nh.value, hit_capacity)].copy(), stats, hist[:, :self.bins], lat.value,
-                             st == _lib.PP_ERR_OVERFLOW)
+        with self._hitbuf_lock:
+            if self._hitbuf is None or len(self._hitbuf) < hit_capacity:
+                self._hitbuf = np.empty(hit_capacity, dtype=_lib.HIT32_DTYPE)
+            hits = self._hitbuf
+            st = self._L.pp_server_result(self._h, rid, hits.ctypes.data, hit_capacity, ctypes.byref(nh),
+                                          stats.ctypes.data, hist.ctypes.data, ctypes.byref(lat))
+            if st not in (_lib.PP_OK, _lib.PP_ERR_OVERFLOW):
+                _lib.check(st)
+            hits = hits[:min(nh.value, hit_capacity)].copy()
+        return RequestResult(hits, stats, hist[:, :self.bins], lat.value, st == _lib.PP_ERR_OVERFLOW)
 
     def counters(self) -> dict:
         c = _lib.ServerCounters()
