@@ -352,6 +352,25 @@ def test_invalid_arguments_raise(propagator):
     q["radius"] = 0
     with pytest.raises(pp.PPError):
         propagator.propagate(q, pp.RunOptions())
+    # the limits of the Philox counter: photon index < 2^40, step < 2^24 - 1
+    q = p.copy()
+    q["n_photons"] = (1 << 40) + 1
+    with pytest.raises(pp.PPError, match="2\\^40"):
+        propagator.propagate(q, pp.RunOptions())
+    with pytest.raises(pp.PPError, match="max_steps"):
+        propagator.propagate(p, pp.RunOptions(max_steps=(1 << 24) - 1))
+    r = propagator.propagate(p, pp.RunOptions(max_steps=(1 << 24) - 2))  # the largest accepted
+    np.testing.assert_array_equal(r.stats[:, 6], p["n_photons"])
+    q = p.copy()
+    q["emitter"] = 7
+    with pytest.raises(pp.PPError, match="unknown emitter"):
+        propagator.propagate(q, pp.RunOptions())
+    q = cone.copy()
+    q["dir"] = (0.0, 0.0, 2.0)
+    with pytest.raises(pp.PPError, match="unit direction"):
+        propagator.propagate(q, pp.RunOptions())
+    with pytest.raises(pp.PPError, match="t_max"):
+        propagator.propagate(p, pp.RunOptions(t_max=float("inf")))
 
 
 def test_device_api_graph_replay_matches_host_api(propagator):
