@@ -10,7 +10,9 @@ loop (pp_propagate called per request, in arrival order, by one worker).
 """
 from __future__ import annotations
 
+import contextlib
 import ctypes
+import gc
 import threading
 import time
 from dataclasses import dataclass
@@ -122,6 +124,21 @@ def _percentiles(lat):
             "p99.9_ms": float(np.percentile(a, 99.9) * 1e3), "max_ms": float(a[-1] * 1e3)}
 
 
+@contextlib.contextmanager
+def _gc_paused():
+    """Python's cyclic garbage collector paused for a timed stream: a full
+    collection walks every result kept so far and can hold the interpreter
+    lock for tens of milliseconds, which would show up as submission delay."""
+    was = gc.isenabled()
+    gc.collect()
+    gc.disable()
+    try:
+        yield
+    finally:
+        if was:
+            gc.enable()
+
+
 def run_open_loop(server: Server, arrivals, reqs, timeout_s=120.0):
     """Submits each request at its arrival time (open loop) from this thread and
     collects results on a second thread.  Latency = completion - scheduled
@@ -138,17 +155,18 @@ def run_open_loop(server: Server, arrivals, reqs, timeout_s=120.0):
             results[i] = server.result(ids[i], timeout_s)
 
     th = threading.Thread(target=collect)
-    th.start()
-    t0 = time.perf_counter()
-    for i, (t, r) in enumerate(zip(arrivals, reqs)):
-        dt = t0 + t - time.perf_counter()
-        if dt > 0:
-            time.sleep(dt)
-        late[i] = max(0.0, time.perf_counter() - (t0 + t))
-        ids[i] = server.submit(r)
-        submitted.release()
-    th.join()
-    wall = time.perf_counter() - t0
+    with _gc_paused():
+        th.start()
+        t0 = time.perf_counter()
+        for i, (t, r) in enumerate(zip(arrivals, reqs)):
+            dt = t0 + t - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            late[i] = max(0.0, time.perf_counter() - (t0 + t))
+            ids[i] = server.submit(r)
+            submitted.release()
+        th.join()
+        wall = time.perf_counter() - t0
     photons = float(sum(int(r["n_photons"].sum()) for r in reqs))
     lat = [x.latency_s + d for x, d in zip(results, late)]
     out = {"requests": len(reqs), "photons": photons, "wall_s": wall, "photons_per_s": photons / wall,
@@ -163,15 +181,16 @@ def run_plain_loop(prop: Propagator, opts: RunOptions, arrivals, reqs, hit_capac
     latency = completion - arrival."""
     o = RunOptions(**{**opts.__dict__})
     o.write_hits = True
-    t0 = time.perf_counter()
     lat = []
-    for t, r in zip(arrivals, reqs):
-        dt = t0 + t - time.perf_counter()
-        if dt > 0:
-            time.sleep(dt)
-        prop.propagate(r, o, hit_capacity=hit_capacity)
-        lat.append(time.perf_counter() - (t0 + t))
-    wall = time.perf_counter() - t0
+    with _gc_paused():
+        t0 = time.perf_counter()
+        for t, r in zip(arrivals, reqs):
+            dt = t0 + t - time.perf_counter()
+            if dt > 0:
+                time.sleep(dt)
+            prop.propagate(r, o, hit_capacity=hit_capacity)
+            lat.append(time.perf_counter() - (t0 + t))
+        wall = time.perf_counter() - t0
     photons = float(sum(int(r["n_photons"].sum()) for r in reqs))
     out = {"requests": len(reqs), "photons": photons, "wall_s": wall, "photons_per_s": photons / wall}
     out.update(_percentiles(lat))
