@@ -264,27 +264,6 @@ __device__ __forceinline__ bool group_all(int g, bool v) {
   return r != 0;
 }
 
-// tile_gemm for one group: its 128 threads' shared-memory writes are fenced
-// and synced, its first thread issues the MMAs into the group's columns.
-__device__ __forceinline__ bool group_gemm(const __nv_bfloat16* a, const __nv_bfloat16* b, uint32_t tmem,
-                                           uint32_t mbar, uint32_t& parity, int g, int gt) {
-  fence_async_smem();
-  tc_fence_before();
-  group_sync(g);
-  tc_fence_after();
-  if (gt == 0) {
-    const uint32_t sa = smem_u32(a), sb = smem_u32(b);
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-      mma_128x128x16(tmem, smem_desc(sa + k * 256, 128, 2048), smem_desc(sb + k * 256, 128, 2048), k > 0);
-    mma_commit(mbar);
-  }
-  const bool ok = group_all(g, mbar_wait(mbar, parity));
-  parity ^= 1u;
-  tc_fence_after();
-  return ok;
-}
-
 // The group's MMAs of one layer; kind 1: x (128 x 16) W1^T, one MMA (the
 // bias rides in K columns 4 and 5: x has ones there, W1 the bias split into
 // BF16 hi and lo); kind 2: h (128 x 128) W^T, eight MMAs, then a ninth,
