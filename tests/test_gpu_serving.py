@@ -83,6 +83,8 @@ def test_wait_is_bounded_and_overflow_is_reported(propagator):
 def test_open_loop_latency(propagator):
     arrivals, reqs = serving.requests(rate_hz=200.0, duration_s=2.0, seed=7)
     with serving.Server(propagator, OPTS) as srv:
+        w_arr, w_req = serving.requests(rate_hz=200.0, duration_s=0.5, seed=8)
+        serving.run_open_loop(srv, w_arr, w_req)  # warm-up: first launches and graph set-up
         out, res = serving.run_open_loop(srv, arrivals, reqs)
     print("open loop", out)
     assert out["requests"] == len(reqs) and out["overflow_requests"] == 0
