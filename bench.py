@@ -161,7 +161,7 @@ class CpuArm:
     work, so its photon mix (emitters, distances, photons per pair) follows the
     batch's."""
 
-    def __init__(self, seed, n_pairs, run_kw):
+    def __init__(self, seed, n_pairs, run_kw, max_photons=0):
         from oracle import batches as ob
         from oracle import oracle as O
         from oracle import tables as tb
@@ -171,6 +171,8 @@ class CpuArm:
         self.T = O.make_tables(m, knots, pmt=ob.pmt_table())
         self.n_pairs = n_pairs
         self.batch = ob.mixed_batch(n_pairs, seed=seed)
+        if max_photons > 0:  # the GPU arm's --max-photons cap
+            self.batch["n_photons"] = np.minimum(self.batch["n_photons"], max_photons)
         self.oo = O.make_opts(mode=O.MODE_PHYSICAL, g=float(np.float32(run_kw["g"])), t_max=run_kw["t_max"],
                               hist_t0=run_kw["hist_t0"], hist_bin_width=run_kw["hist_bin_width"],
                               hist_bins=run_kw["hist_bins"], flags=O.OPT_PMT_WEIGHT)
@@ -200,9 +202,9 @@ class CpuArm:
                           f"chunks, {used} threads ran (host has {self.cores})"}
 
 
-def cpu_baseline(seed, n_pairs, target_seconds, run_kw):
+def cpu_baseline(seed, n_pairs, target_seconds, run_kw, max_photons=0):
     """One calibrated CPU pass of about target_seconds (see CpuArm)."""
-    arm = CpuArm(seed, n_pairs, run_kw)
+    arm = CpuArm(seed, n_pairs, run_kw, max_photons)
     arm.calibrate(target_seconds)
     return arm.describe(*arm.run())
 
@@ -783,7 +785,7 @@ def run_reference(args):
         return
     steps, warm = args.steps, args.warmup
     seed = args.seed + warm  # the GPU arm's first timed batch (rank 0)
-    arm = CpuArm(seed, args.pairs, RUN_KW)
+    arm = CpuArm(seed, args.pairs, RUN_KW, args.max_photons)
     per_step = max(1.0, min(args.cpu_seconds, 90.0 / max(steps + warm, 1)))
     arm.calibrate(per_step)
     photons = []
@@ -1076,9 +1078,11 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(args.seed + W, n_pairs, args.cpu_seconds, RUN_KW)
+        cpu = cpu_baseline(args.seed + W, n_pairs, args.cpu_seconds, RUN_KW, args.max_photons)
         from oracle import batches as ob
         ob_batch = ob.mixed_batch(n_pairs, seed=args.seed + W)
+        if args.max_photons > 0:
+            ob_batch["n_photons"] = np.minimum(ob_batch["n_photons"], args.max_photons)
         cpu["same_batch_as_gpu"] = bool(np.array_equal(ob_batch["n_photons"], batches[W]["n_photons"])
                                         and np.array_equal(ob_batch["seed"], batches[W]["seed"])
                                         and np.array_equal(ob_batch["target"], batches[W]["target"]))
