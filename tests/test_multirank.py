@@ -52,7 +52,7 @@ def _gpu_fn():
     return fn
 
 
-def _worker(rank, world, port, out_dir, use_gpu=False):
+def _worker(rank, world, port, out_dir, use_gpu=False, backend="gloo"):
     import sys
     repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
     sys.path[:0] = [repo, os.path.join(repo, "photonprop.jl_b200")]
@@ -62,10 +62,18 @@ def _worker(rank, world, port, out_dir, use_gpu=False):
     from photonprop_b200.parallel import propagate_sharded
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
-    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    device = None
+    if backend == "nccl":  # the exchange's tensors on the GPU
+        import torch
+        torch.cuda.set_device(0)
+        device = torch.device("cuda", 0)
+        dist.init_process_group("nccl", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60),
+                                device_id=device)
+    else:
+        dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     pairs = pp.batches.mixed_batch(24, seed=123, n_min=1e4, n_max=1e5, d_min=2.0, d_max=6.0)
     opts = pp.RunOptions(mode="physical", t_max=200.0, hist_bins=200)
-    res = propagate_sharded(pairs, opts, _gpu_fn() if use_gpu else _oracle_fn())
+    res = propagate_sharded(pairs, opts, _gpu_fn() if use_gpu else _oracle_fn(), device=device)
     np.savez(os.path.join(out_dir, f"rank{rank}.npz"), stats=res.stats, hist=res.hist, hits=res.hits.view(np.uint8),
              n_hits=res.n_hits)
     dist.barrier()
@@ -84,17 +92,18 @@ def test_shard_pairs_balanced_and_disjoint():
         assert loads.max() / loads.mean() < 1.01
 
 
-def _two_ranks(tmp_path, use_gpu):
+def _two_ranks(tmp_path, use_gpu, world=2, backend="gloo"):
     import torch.multiprocessing as mp
     port = _free_port()
-    mp.start_processes(_worker, args=(2, port, str(tmp_path), use_gpu), nprocs=2, join=True, start_method="spawn")
+    mp.start_processes(_worker, args=(world, port, str(tmp_path), use_gpu, backend), nprocs=world, join=True,
+                       start_method="spawn")
     import photonprop_b200 as pp
     pairs = pp.batches.mixed_batch(24, seed=123, n_min=1e4, n_max=1e5, d_min=2.0, d_max=6.0)
     opts = pp.RunOptions(mode="physical", t_max=200.0, hist_bins=200)
     ref = _gpu_fn()(pairs, opts) if use_gpu else _oracle_fn()(pairs, opts)
     # FP64 atomics add in any order on the GPU: equal to rounding there, bit for bit on the oracle
     rtol = 1e-12 if use_gpu else 0.0
-    for r in range(2):
+    for r in range(world):
         d = np.load(tmp_path / f"rank{r}.npz")
         np.testing.assert_allclose(d["stats"], ref.stats, rtol=rtol, atol=0)
         np.testing.assert_allclose(d["hist"], ref.hist, rtol=rtol, atol=0)
@@ -112,6 +121,14 @@ def test_two_rank_gloo_matches_single_process(tmp_path):
 @pytest.mark.gpu
 def test_two_rank_gloo_gpu_shards_match_single_process(tmp_path):
     ref = _two_ranks(tmp_path, use_gpu=True)
+    assert ref.n_hits > 100
+
+
+@pytest.mark.gpu
+def test_one_rank_nccl_device_exchange_matches_single_process(tmp_path):
+    """The exchange with its tensors on the GPU over NCCL (one rank: this
+    run has one GPU, and two ranks of NCCL on one GPU are not allowed)."""
+    ref = _two_ranks(tmp_path, use_gpu=True, world=1, backend="nccl")
     assert ref.n_hits > 100
 
 
