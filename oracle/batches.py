@@ -9,7 +9,7 @@ them) and ``pair_seed`` is splitmix64 (Steele, Lea, Flood, OOPSLA 2014) of
 seed + golden-ratio * (index + 1), the product's per-pair seed; a CPU test
 checks both against the product field by field.
 
-The workload is the batched configuration of the north-star benchmark: photon
+The workload is the 4096-pair mixed-batch benchmark: photon
 counts log-uniform in [1e4, 1e7], 50/50 isotropic point / 1 m Cherenkov-cone
 emitters with directions uniform on the sphere, sphere centres at a uniform
 distance in [2, 150] m in a random direction, radius 0.21 m.  The reference
