@@ -116,7 +116,7 @@ typedef struct {
   float target[3];   /* sphere centre */
   float radius;      /* sphere radius */
   int64_t n_photons; /* photons to propagate */
-  uint64_t seed;     /* Philox key; the stream depends only on (seed, photon) */
+  uint64_t seed;     /* random stream: depends only on (seed, photon) */
   int32_t emitter;   /* PP_EMITTER_* */
   int32_t reserved[3];
 } pp_pair;
@@ -538,7 +538,9 @@ PP_API pp_status pp_autotune(pp_ctx* ctx, const pp_pair* pairs, int64_t n_pairs,
  * 4 update_position (in: pos[3],dir[3],step; out: 3), 5 equidistant
  * interpolation of the context's knots (in: u), 6 refractive index,
  * 7 group index, 8 scattering length, 9 absorption length, 10 PMT
- * acceptance (in: wavelength), 11 cascade-emitter cos theta (in: u, n). */
+ * acceptance (in: wavelength), 11 cascade-emitter cos theta (in: u, n),
+ * 12 a step's Philox2x32-10 block and its three uniforms (in: counter
+ * words 0, 1 and the key; out: w0, w1, u0, u1, u2). */
 PP_API pp_status pp_device_eval(pp_ctx* ctx, int32_t op, const double* in, double* out, int64_t n);
 
 /* Measures this device's FP32 FMA and MUFU (transcendental) issue peaks with
@@ -549,7 +551,7 @@ PP_API pp_status pp_measure_peaks(int device, double* fp32_ops_per_s, double* mu
 
 /* Speed of light of the physical photon step on this device: photon steps
  * per second when every lane of every SM steps its own photon (one
- * Philox4x32-10 block, ray-sphere test, move, Henyey-Greenstein turn) with no
+ * Philox2x32-10 block, ray-sphere test, move, Henyey-Greenstein turn) with no
  * emission, refill, hit record or loop bookkeeping, at the batched kernel's
  * occupancy.  No reference counterpart: the ceiling the batched kernel's
  * step rate is reported against. */

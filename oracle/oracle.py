@@ -75,6 +75,8 @@ def lib():
         dp = ctypes.POINTER(ctypes.c_double)
         u32p = ctypes.POINTER(ctypes.c_uint32)
         L.orc_philox4x32_10.argtypes = [u32p, u32p, u32p]
+        L.orc_philox2x32_10.argtypes = [u32p, ctypes.c_uint32, u32p]
+        L.orc_step_uniforms.argtypes = [u32p, ctypes.POINTER(ctypes.c_double)]
         L.orc_uniform.argtypes = [ctypes.c_uint32]
         L.orc_uniform.restype = ctypes.c_double
         L.orc_hg_costheta.argtypes = [ctypes.c_double, ctypes.c_double]
@@ -111,6 +113,21 @@ def philox4x32_10(ctr, key):
     o = (ctypes.c_uint32 * 4)()
     lib().orc_philox4x32_10(c, k, o)
     return list(o)
+
+
+def philox2x32_10(ctr, key):
+    c = (ctypes.c_uint32 * 2)(*ctr)
+    o = (ctypes.c_uint32 * 2)()
+    lib().orc_philox2x32_10(c, int(key) & 0xFFFFFFFF, o)
+    return list(o)
+
+
+def step_uniforms(w):
+    """The three 21-bit uniforms of a step from its Philox2x32 block (w0, w1)."""
+    c = (ctypes.c_uint32 * 2)(*w)
+    u = (ctypes.c_double * 3)()
+    lib().orc_step_uniforms(c, u)
+    return list(u)
 
 
 def uniform(w):

@@ -11,11 +11,14 @@
  *   - arrival time t = t_emit + dist * n_group(lambda) / c;
  *   - a photon ends when its next position would lie beyond the time window
  *     t_max, when it hits the sphere, or after max_steps steps.
- * Random numbers: Philox4x32-10 (Salmon et al., SC'11) under the fixed key
- * (0x243F6A88, 0x85A308D3) with counter (seed lo, seed hi, photon lo,
- * photon hi | block << 8) for a photon index below 2^40.  Block 0 gives the
- * emission draws (wavelength, polar angle or track position, azimuth), block
- * k+1 the draws of step k (step length, HG cos(theta), azimuth).
+ * Random numbers (Salmon et al., SC'11).  Emission: Philox4x32-10 under the
+ * fixed key (0x243F6A88, 0x85A308D3) with counter (seed lo, seed hi,
+ * photon lo, photon hi) for a photon index below 2^40; its words w0..w2 give
+ * the emission draws (wavelength, polar angle or track position, azimuth) as
+ * 23-bit uniforms.  Steps: the photon's own Philox2x32-10 stream, keyed by
+ * w3, with counter (the low 9 bits of w0, w1, w2 packed into 27 bits,
+ * photon hi | (k + 1) << 8) for step k; its 64 output bits give three 21-bit
+ * uniforms (step length, HG cos(theta), azimuth).
  */
 #include "pp_oracle.h"
 
@@ -55,6 +58,36 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
   out[1] = c1;
   out[2] = c2;
   out[3] = c3;
+}
+
+/* Philox2x32-10 (same paper): multiplier 0xD256D193, Weyl key increment
+ * 0x9E3779B9. */
+void orc_philox2x32_10(const uint32_t ctr[2], uint32_t key, uint32_t out[2]) {
+  uint32_t c0 = ctr[0], c1 = ctr[1], k = key;
+  for (int r = 0; r < 10; ++r) {
+    if (r) k += 0x9E3779B9u;
+    uint64_t p = (uint64_t)0xD256D193u * c0;
+    uint32_t n0 = (uint32_t)(p >> 32) ^ c1 ^ k;
+    c0 = n0;
+    c1 = (uint32_t)p;
+  }
+  out[0] = c0;
+  out[1] = c1;
+}
+
+/* The three 21-bit uniforms of a step from the 64 bits (w0, w1) of its
+ * Philox2x32 block: bits 63..43, 42..22 and 21..1 of w0:w1, each as
+ * (k + 1/2) * 2^-21 (exact in FP32). */
+void orc_step_uniforms(const uint32_t w[2], double u[3]) {
+  const uint64_t b = ((uint64_t)w[0] << 32) | w[1];
+  for (int i = 0; i < 3; ++i) u[i] = ((double)((b >> (43 - 21 * i)) & 0x1FFFFFu) + 0.5) * (1.0 / 2097152.0);
+}
+
+/* The step stream of a photon from its emission block: key w3, counter word
+ * 0 the low 9 bits of w0, w1 and w2. */
+void orc_step_stream(const uint32_t w[4], uint32_t* key, uint32_t* word0) {
+  *key = w[3];
+  *word0 = (w[0] & 0x1FFu) | ((w[1] & 0x1FFu) << 9) | ((w[2] & 0x1FFu) << 18);
 }
 
 /* 23-bit uniform in the open interval (0, 1): ((w >> 9) + 1/2) * 2^-23.
@@ -159,13 +192,23 @@ static void hb_push(hitbuf* b, const orc_hit* h) {
   b->h[b->n++] = *h;
 }
 
-static void philox_block(uint64_t seed, int64_t photon, uint32_t block, double u[4]) {
+/* Emission block of a photon: its three uniforms and the step stream. */
+static void emission_block(uint64_t seed, int64_t photon, double u[3], uint32_t* skey, uint32_t* sword) {
   uint32_t key[2] = {ORC_KEY0, ORC_KEY1};
   uint32_t ctr[4] = {(uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)(uint64_t)photon,
-                     (uint32_t)((uint64_t)photon >> 32) | (block << 8)};
+                     (uint32_t)((uint64_t)photon >> 32)};
   uint32_t w[4];
   orc_philox4x32_10(ctr, key, w);
-  for (int i = 0; i < 4; ++i) u[i] = orc_uniform(w[i]);
+  for (int i = 0; i < 3; ++i) u[i] = orc_uniform(w[i]);
+  orc_step_stream(w, skey, sword);
+}
+
+/* Uniforms of step k of a photon. */
+static void step_block(uint32_t skey, uint32_t sword, int64_t photon, int k, double u[3]) {
+  uint32_t ctr[2] = {sword, (uint32_t)((uint64_t)photon >> 32) | ((uint32_t)(k + 1) << 8)};
+  uint32_t w[2];
+  orc_philox2x32_10(ctr, skey, w);
+  orc_step_uniforms(w, u);
 }
 
 /* cos(theta) of the cascade emitter: inverse CDF of the EM-cascade profile
@@ -193,8 +236,9 @@ static double cascade_cos_theta(const orc_tables* T, double c0, double u) {
 static int simulate_photon(const orc_tables* T, const orc_pair* P, int64_t pair_idx, int64_t ph,
                            const orc_opts* O, orc_hit* out, int64_t* steps) {
   const int compat = (O->mode == 0);
-  double u[4];
-  philox_block(P->seed, ph, 0u, u);
+  double u[3];
+  uint32_t skey, sword;
+  emission_block(P->seed, ph, u, &skey, &sword);
   /* initialize_wavelength, src/photon_prop_cuda.jl:73-75 */
   double wl = (T->n_knots == 1) ? T->knots[0] : orc_interp_equidistant(u[0], T->knots, T->n_knots, 0.0, 1.0);
   double phi = ORC_TWO_PI * u[2]; /* uniform(0, 2pi), :54 */
@@ -238,7 +282,7 @@ static int simulate_photon(const orc_tables* T, const orc_pair* P, int64_t pair_
   double rsq = P->radius * P->radius;
   for (int k = 0; k < O->max_steps; ++k) {
     ++*steps;
-    philox_block(P->seed, ph, (uint32_t)(k + 1), u);
+    step_block(skey, sword, ph, k, u);
     double step = -log(u[0]) * sca_len; /* :322-323 */
     double a = 0.0, pp = 0.0;           /* :330-337 */
     for (int j = 0; j < 3; ++j) {

@@ -3,12 +3,13 @@
  *
  * TEST INFRASTRUCTURE ONLY: a restatement of the reference kernel
  * cuda_propagate_photons! (src/photon_prop_cuda.jl:262-386) and its helpers,
- * replaying the same Philox4x32-10 random numbers as the CUDA kernels.  Only
+ * replaying the same Philox random numbers as the CUDA kernels (a photon's
+ * emission block is Philox4x32-10, its steps its own Philox2x32-10 stream).  Only
  * the tests, the smoke check and the CPU-baseline leg of bench.py load it, and
  * only as the checker.  Nothing in the product links it.
  *
  * Parity status: the helper functions are pinned by the known-answer tests of
- * src/tests/test_photon_prob.jl and Philox by the Random123 known-answer
+ * src/tests/test_photon_prob.jl and both Philox forms by the Random123 known-answer
  * vectors; end-to-end hit statistics are "parity unpinned" against the
  * reference itself (the reference is Julia/CUDA.jl and cannot run here, and
  * its device RNG stream is not reproducible).
@@ -81,6 +82,9 @@ typedef struct {
 #define ORC_STATS 8
 
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+void orc_philox2x32_10(const uint32_t ctr[2], uint32_t key, uint32_t out[2]);
+void orc_step_uniforms(const uint32_t w[2], double u[3]);
+void orc_step_stream(const uint32_t w[4], uint32_t* key, uint32_t* word0);
 double orc_uniform(uint32_t w);
 double orc_hg_costheta(double g, double u);
 void orc_rotate_to_axis(const double old_dir[3], const double new_dir[3], double out[3]);

@@ -742,9 +742,9 @@ pp_status pp_cuda_propagate_photons(pp_ctx* c, float* pos, float* dir, float* wl
 pp_status pp_device_eval(pp_ctx* c, int32_t op, const double* in, double* out, int64_t n) {
   if (!c) return PP_ERR_ARG;
   std::lock_guard<std::mutex> lk(c->mu);
-  static const int in_w[] = {6, 1, 2, 6, 7, 1, 1, 1, 1, 1, 1, 2};
-  static const int out_w[] = {4, 1, 1, 3, 3, 1, 1, 1, 1, 1, 1, 1};
-  if (op < 0 || op > 11 || n < 0 || (n > 0 && (!in || !out))) return c->fail(PP_ERR_ARG, "pp_device_eval: bad arguments");
+  static const int in_w[] = {6, 1, 2, 6, 7, 1, 1, 1, 1, 1, 1, 2, 3};
+  static const int out_w[] = {4, 1, 1, 3, 3, 1, 1, 1, 1, 1, 1, 1, 5};
+  if (op < 0 || op > 12 || n < 0 || (n > 0 && (!in || !out))) return c->fail(PP_ERR_ARG, "pp_device_eval: bad arguments");
   if (n == 0) return PP_OK;
   DeviceGuard guard(c->device);
   double *din = nullptr, *dout = nullptr;

@@ -97,8 +97,27 @@ __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k
   }
 }
 
-struct Draw4 {
-  float u0, u1, u2, u3;
+// Philox2x32-10 (same paper): one multiplier and one key word, whose Weyl
+// increments are added per round (the key varies per photon).  A block gives
+// 64 bits for two 32x32 products per round, against 128 bits for four in a
+// Philox4x32 block; a step needs 63 bits.
+__host__ __device__ __forceinline__ void philox2x32_10(uint32_t& c0, uint32_t& c1, uint32_t k) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+#ifdef __CUDA_ARCH__
+    const uint32_t h = __umulhi(c0, 0xD256D193u), l = c0 * 0xD256D193u;
+#else
+    const uint64_t p = (uint64_t)c0 * 0xD256D193u;
+    const uint32_t h = (uint32_t)(p >> 32), l = (uint32_t)p;
+#endif
+    c0 = h ^ k ^ c1;
+    c1 = l;
+    k += 0x9E3779B9u;
+  }
+}
+
+struct Draw3 {
+  float u0, u1, u2;
 };
 
 // ((w >> 9) + 1/2) * 2^-23, exact in FP32: 1.m - (1 - 2^-24).  The mantissa
@@ -114,15 +133,36 @@ __device__ __forceinline__ float u01(uint32_t w) {
 constexpr uint32_t kKey0 = 0x243F6A88u;  // fixed Philox key (hex digits of pi)
 constexpr uint32_t kKey1 = 0x85A308D3u;
 
-// Counter word 3: photon index bits 32..39 and the block number above them.
+// Photon index bits 32..39 and a step's block number (step k: k + 1) above
+// them: word 3 of the emission counter (block 0) and word 1 of the step
+// counter.
 __device__ __forceinline__ uint32_t ctr_word(uint64_t photon, uint32_t block) {
   return (uint32_t)(photon >> 32) | (block << 8);
 }
 
-__device__ __forceinline__ Draw4 draw_block(uint32_t seed_lo, uint32_t seed_hi, uint64_t photon, uint32_t word3) {
-  uint32_t c[4] = {seed_lo, seed_hi, (uint32_t)photon, word3};
+// Emission block of a photon: Philox4x32-10 under the fixed key with counter
+// (seed lo, seed hi, photon lo, photon hi).  Words 0..2 give the emission's
+// uniforms (their top 23 bits), word 3 and the low 9 bits of words 0..2 the
+// key and counter word 0 of the photon's step stream.
+__device__ __forceinline__ uint4 emission_block(uint32_t seed_lo, uint32_t seed_hi, uint64_t photon) {
+  uint32_t c[4] = {seed_lo, seed_hi, (uint32_t)photon, ctr_word(photon, 0u)};
   philox4x32_10(c, kKey0, kKey1);
-  return Draw4{u01(c[0]), u01(c[1]), u01(c[2]), u01(c[3])};
+  return make_uint4(c[0], c[1], c[2], c[3]);
+}
+__device__ __forceinline__ Draw3 emission_uniforms(const uint4& w) { return Draw3{u01(w.x), u01(w.y), u01(w.z)}; }
+__device__ __forceinline__ uint32_t step_word0(const uint4& w) {
+  return (w.x & 0x1FFu) | ((w.y & 0x1FFu) << 9) | ((w.z & 0x1FFu) << 18);
+}
+
+// A step's three uniforms from its Philox2x32 block (w0, w1): bits 63..43,
+// 42..22 and 21..1 of w0:w1, each placed in mantissa bits 22..2 of 1.m with
+// bit 1 set, so that 1.m - 1 = (k + 1/2) 2^-21 exactly.
+__device__ __forceinline__ Draw3 step_uniforms(uint32_t w0, uint32_t w1) {
+  const uint32_t m0 = (w0 >> 9) & 0x7FFFFCu;
+  const uint32_t m1 = __funnelshift_r(w1, w0, 20) & 0x7FFFFCu;
+  const uint32_t m2 = (w1 << 1) & 0x7FFFFCu;
+  return Draw3{__uint_as_float(m0 | 0x3F800002u) - 1.f, __uint_as_float(m1 | 0x3F800002u) - 1.f,
+               __uint_as_float(m2 | 0x3F800002u) - 1.f};
 }
 
 // ---- resident tables (one copy per context, staged into shared memory) ----
@@ -288,6 +328,8 @@ struct Photon {
   float path;         // physical: path left before t_max; compat: path travelled
   float neg_ln2_len;  // -ln2 * scattering length: step = lg2(u) * this
   uint32_t ctr3;      // Philox counter word of the next event: block (= steps + 1) << 8 | photon bits 32..39
+  uint32_t skey;      // the step stream's Philox2x32 key and counter word 0 (from the emission block)
+  uint32_t sword;
   uint64_t id;
 };
 
@@ -336,7 +378,7 @@ enum { kEmBasic = 0, kEmCascade = 1 };
 
 template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ EmissionFrame emission_frame(const DevTables& T, const pp_pair* __restrict__ P,
-                                                        const Draw4& d) {
+                                                        const Draw3& d) {
   const float4 pt = __ldg(reinterpret_cast<const float4*>(P));      // pos, t0
   const float4 dl = __ldg(reinterpret_cast<const float4*>(P) + 1);  // dir, track_len
   const int emitter = __ldg(reinterpret_cast<const int*>(P) + 16);
@@ -415,12 +457,14 @@ __device__ __forceinline__ float path_at_tmax(const DevTables& T, const RunParam
   return (R.t_max - f.t_emit) * kCVac * rcp(group_index(T, rcp(f.wl)));
 }
 
-// Emission of photon s.id (block 0): position, direction and the
-// per-wavelength constants; afterwards the next event is block 1.
+// Emission of photon s.id (its emission block): position, direction, the
+// per-wavelength constants and the step stream; afterwards the next event
+// is step 0 (step block 1).
 template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                            const PairCtx& c, Photon& s) {
-  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, ctr_word(s.id, 0u));
+  const uint4 w = emission_block(c.seed_lo, c.seed_hi, s.id);
+  const Draw3 d = emission_uniforms(w);
   const EmissionFrame f = emission_frame<MODE, EM>(T, P, d);
   const float3 tg = pair_target(P);
   s.px = f.px - tg.x;
@@ -429,16 +473,21 @@ __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& 
   s.path = (MODE == kPhysical) ? path_at_tmax(T, R, f) : 0.f;
   s.neg_ln2_len = -kLn2 * scattering_length(T, f.wl);
   emission_direction(f, d.u2, s.dx, s.dy, s.dz);
+  s.skey = w.w;
+  s.sword = step_word0(w);
   s.ctr3 = ctr_word(s.id, 1u);
 }
 
-// Step k (block k + 1) of src/photon_prop_cuda.jl:320-376: step length,
+// Step k (block k + 1 of the photon's Philox2x32 stream) of
+// src/photon_prop_cuda.jl:320-376: step length,
 // ray-sphere test, move, Henyey-Greenstein turn.  Returns false when the
 // photon ends; *hit is set when it ends on the sphere (position and path
 // length then at the hit).
 template <int MODE>
 __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c, Photon& s, bool& hit) {
-  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, s.ctr3);
+  uint32_t w0 = s.sword, w1 = s.ctr3;
+  philox2x32_10(w0, w1, s.skey);
+  const Draw3 d = step_uniforms(w0, w1);
   const float step = lg2(d.u0) * s.neg_ln2_len;
   const float ex = s.px, ey = s.py, ez = s.pz;  // photon - sphere centre
   const float a = fmaf(s.dz, ez, fmaf(s.dy, ey, s.dx * ex));
@@ -507,7 +556,7 @@ struct HitValues {
 template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ HitValues hit_values(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                                 const PairCtx& c, const Photon& s) {
-  const Draw4 d = draw_block(c.seed_lo, c.seed_hi, s.id, ctr_word(s.id, 0u));
+  const Draw3 d = emission_uniforms(emission_block(c.seed_lo, c.seed_hi, s.id));
   const EmissionFrame f = emission_frame<MODE, EM>(T, P, d);
   HitValues h;
   h.wl = f.wl;

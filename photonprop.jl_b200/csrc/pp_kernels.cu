@@ -36,8 +36,8 @@ struct __align__(16) Staged {
   float px, py, pz, dx, dy, dz, neg_ln2_len, path;
   uint32_t id_lo, id_hi;
   int32_t pair;
-  float radius;              // the pair's sphere radius and seed, so that a
-  uint32_t seed_lo, seed_hi;  // refill reads shared memory only
+  float radius;         // the pair's sphere radius, so that a refill reads
+  uint32_t skey, sword;  // shared memory only, and the photon's step stream
   uint32_t pad[2];
 };
 
@@ -95,6 +95,7 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
       p.neg_ln2_len = 0.f;
       p.id = ((unsigned long long)g.id_hi << 32) | g.id_lo;
       p.ctr3 = 0u;
+      p.skey = p.sword = 0u;
       const PairCtx pc = load_pair_ctx(R.pairs + g.pair, g.pair);
       const HitValues h = hit_values<MODE, EM>(T, R, R.pairs + g.pair, pc, p);
       record_hit_cached(R, ws, pc, p, h);
@@ -114,8 +115,11 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
   Photon s;
   s.id = 0;
   s.ctr3 = 1u << 8;
+  s.skey = s.sword = 0u;
   s.px = s.py = s.pz = s.dx = s.dy = s.path = s.neg_ln2_len = 0.f;
   s.dz = 1.f;
+  // the lane's pair: radius and index (the seed, which only a hit's emission
+  // replay needs, is read from the pair record then)
   PairCtx c;
   c.r = 0.f;
   c.seed_lo = c.seed_hi = 0u;
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         dst[1] = make_float4(e.dy, e.dz, e.neg_ln2_len, e.path);
         dst[2] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)),
                              __int_as_float(ppair), pc.r);
-        dst[3] = make_float4(__uint_as_float(pc.seed_lo), __uint_as_float(pc.seed_hi), 0.f, 0.f);
+        dst[3] = make_float4(__uint_as_float(e.skey), __uint_as_float(e.sword), 0.f, 0.f);
       }
       r_count += filled;
       __syncwarp();
@@ -209,8 +213,8 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         s.ctr3 = ctr_word(s.id, 1u);
         c.index = __float_as_int(d.z);
         c.r = d.w;
-        c.seed_lo = __float_as_uint(e.x);
-        c.seed_hi = __float_as_uint(e.y);
+        s.skey = __float_as_uint(e.x);
+        s.sword = __float_as_uint(e.y);
         alive = true;
       }
     }
@@ -254,8 +258,9 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
       }
     } else if (__any_sync(kFull, hit)) {
       if (hit) {
-        const HitValues h = hit_values<MODE, EM>(T, R, R.pairs + c.index, c, s);
-        record_hit_cached(R, ws, c, s, h);
+        const PairCtx pc = load_pair_ctx(R.pairs + c.index, c.index);
+        const HitValues h = hit_values<MODE, EM>(T, R, R.pairs + c.index, pc, s);
+        record_hit_cached(R, ws, pc, s, h);
       }
     }
   }
@@ -450,6 +455,19 @@ __global__ void eval_kernel(int op, const double* __restrict__ in, double* __res
       break;
     }
     case 1: out[i] = (double)u01((uint32_t)in[i]); break;
+    case 12: {  // step block: (counter word 0, word 1, key) -> (w0, w1, u0, u1, u2)
+      const double* a = in + 3 * i;
+      uint32_t w0 = (uint32_t)a[0], w1 = (uint32_t)a[1];
+      philox2x32_10(w0, w1, (uint32_t)a[2]);
+      const Draw3 d = step_uniforms(w0, w1);
+      double* o = out + 5 * i;
+      o[0] = (double)w0;
+      o[1] = (double)w1;
+      o[2] = (double)d.u0;
+      o[3] = (double)d.u1;
+      o[4] = (double)d.u2;
+      break;
+    }
     case 2: {
       const float g = (float)in[2 * i];
       HG h;
@@ -534,7 +552,7 @@ __global__ void peak_philox_kernel(unsigned* out, int iters) {
 }
 
 // Speed of light of the physical step: every lane steps its own photon
-// through step_event (one Philox4x32-10 block, the ray-sphere test, the move
+// through step_event (one Philox2x32-10 block, the ray-sphere test, the move
 // and the Henyey-Greenstein turn) with no emission, refill, hit record or
 // loop bookkeeping, at the batched kernel's occupancy (256 threads, 4 CTAs
 // per SM, at most 64 registers).  Its step rate bounds what the batched
@@ -545,10 +563,11 @@ __global__ void __launch_bounds__(256, 4) peak_step_kernel(const RunParams R, in
                                                            unsigned long long* __restrict__ out) {
   PairCtx c;
   c.r = 0.21f;
-  c.seed_lo = 0x9E3779B9u * (blockIdx.x + 1u);
-  c.seed_hi = 0x2545F491u;
+  c.seed_lo = c.seed_hi = 0u;
   c.index = 0;
   Photon s;
+  s.skey = 0x9E3779B9u * (blockIdx.x + 1u);
+  s.sword = 0x2545F491u ^ threadIdx.x;
   s.id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   s.px = 100.f + (float)(threadIdx.x & 31u);
   s.py = 50.f;

@@ -45,7 +45,7 @@ def measure_peaks(device=0):
 
 def measure_step_rate(device=0):
     """Photon steps per second of the bare physical step on every SM (one
-    Philox block, ray-sphere test, move, turn; no emission, refill, hit
+    Philox2x32 block, ray-sphere test, move, turn; no emission, refill, hit
     record or loop bookkeeping): the speed of light of the step loop."""
     import ctypes
     L = _lib.load()

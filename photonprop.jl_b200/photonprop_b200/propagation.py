@@ -239,7 +239,7 @@ class Propagator:
                 "chunk_photons": best.chunk_photons, "photons_per_s": rate.value}
 
     def device_eval(self, op: int, inputs) -> np.ndarray:
-        out_w = {0: 4, 3: 3, 4: 3}.get(op, 1)
+        out_w = {0: 4, 3: 3, 4: 3, 12: 5}.get(op, 1)
         x = np.ascontiguousarray(inputs, dtype=np.float64)
         n = x.shape[0] if x.ndim > 0 else 1
         out = np.zeros((n, out_w))

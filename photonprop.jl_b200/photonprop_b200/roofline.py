@@ -14,9 +14,10 @@ per photon step   7 MUFU  the reference's arithmetic (src/photon_prop_cuda.jl:
                           kernel confirm.
                  ~45 FP32 in the reference's form; this kernel issues 56
                           (ncu: 28 FFMA, 20 FMUL, 8 FADD per step).
-                  1 Philox4x32-10 block.
+                  1 Philox2x32-10 block (20 32x32-bit products: half a
+                          Philox4x32-10 block, as which it is counted).
 per photon start  isotropic: 10 MUFU, 28 FP32; Cherenkov cone: 14 MUFU, 60 FP32;
-                  plus one Philox block.
+                  plus one Philox4x32-10 block.
 A photon that hits the sphere also re-draws its emission block (rare).
 """
 
@@ -24,14 +25,14 @@ MUFU_PER_STEP_ALG = 7
 FP32_PER_STEP_ALG = 45
 MUFU_PER_STEP = 7
 FP32_PER_STEP = 56
-PHILOX_PER_STEP = 1
+PHILOX_PER_STEP = 0.5  # Philox4x32-10 block equivalents (by 32x32-bit products)
 MUFU_PER_PHOTON = {0: 10, 1: 14}   # by emitter type
 FP32_PER_PHOTON = {0: 28, 1: 60}
 PHILOX_PER_PHOTON = 1
 
 
 def op_counts(steps, photons_iso, photons_cone, algorithmic=False):
-    """(mufu, fp32, philox blocks) for a run; algorithmic=True counts the
+    """(mufu, fp32, Philox4x32-10 block equivalents) for a run; algorithmic=True counts the
     step as the reference's arithmetic does, else as this kernel issues it."""
     m_step = MUFU_PER_STEP_ALG if algorithmic else MUFU_PER_STEP
     f_step = FP32_PER_STEP_ALG if algorithmic else FP32_PER_STEP

@@ -3,8 +3,8 @@
 reference_kats.json  known-answer tests of the reference's own test file
                      src/tests/test_photon_prob.jl (values transcribed with
                      their file:line) and the Random123 Philox4x32-10
-                     known-answer vectors (the algorithm the kernels and the
-                     oracle share).
+                     and Philox2x32-10 known-answer vectors (the algorithms
+                     the kernels and the oracle share).
 oracle_golden.json   outputs of the FP64 oracle on small fixed cases (medium
                      spot values, Cherenkov knots, a reference-compatible run
                      and a physical-mode run), so that any change to the
@@ -52,6 +52,13 @@ PHILOX_KATS = [
      "out": [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]},
     {"ctr": [0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], "key": [0xa4093822, 0x299f31d0],
      "out": [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]},
+]
+
+# Random123 kat_vectors, philox2x32 R=10: (counter[2], key) -> out[2]
+PHILOX2_KATS = [
+    {"ctr": [0, 0], "key": 0, "out": [0xff1dae59, 0x6cd10df2]},
+    {"ctr": [0xffffffff, 0xffffffff], "key": 0xffffffff, "out": [0x2c3f628b, 0xab4fd7ad]},
+    {"ctr": [0x243f6a88, 0x85a308d3], "key": 0x13198a2e, "out": [0xdd7ce038, 0xf62a4c12]},
 ]
 
 
@@ -111,7 +118,8 @@ def oracle_golden():
 
 def main():
     with open(os.path.join(HERE, "reference_kats.json"), "w") as f:
-        json.dump({"reference": REFERENCE_KATS, "philox4x32_10": PHILOX_KATS}, f, indent=1)
+        json.dump({"reference": REFERENCE_KATS, "philox4x32_10": PHILOX_KATS, "philox2x32_10": PHILOX2_KATS}, f,
+                  indent=1)
     with open(os.path.join(HERE, "oracle_golden.json"), "w") as f:
         json.dump(oracle_golden(), f, indent=1)
 

@@ -37,6 +37,15 @@ def test_device_philox_and_uniform_bit_exact(propagator):
     w = rng.integers(0, 2**32, size=1000, dtype=np.uint64)
     u = propagator.device_eval(1, w.astype(np.float64))[:, 0]
     np.testing.assert_array_equal(u, [O.uniform(int(x)) for x in w])
+    # a step's Philox2x32-10 block and its three 21-bit uniforms
+    sc = rng.integers(0, 2**32, size=(512, 3), dtype=np.uint64)
+    sc[0] = 0
+    sc[1] = 0xFFFFFFFF
+    out = propagator.device_eval(12, sc.astype(np.float64))
+    for i in range(512):
+        wds = O.philox2x32_10([int(sc[i, 0]), int(sc[i, 1])], int(sc[i, 2]))
+        assert [int(x) for x in out[i, :2]] == wds
+        assert list(out[i, 2:]) == O.step_uniforms(wds)
 
 
 def test_device_hg_costheta(propagator):

@@ -29,6 +29,31 @@ def test_philox_random123_vectors(kat):
     assert O.philox4x32_10(kat["ctr"], kat["key"]) == kat["out"]
 
 
+@pytest.mark.parametrize("kat", KATS["philox2x32_10"])
+def test_philox2x32_random123_vectors(kat):
+    assert O.philox2x32_10(kat["ctr"], kat["key"]) == kat["out"]
+
+
+def test_step_uniforms_bit_fields():
+    # 21-bit fields 63..43, 42..22, 21..1 of w0:w1, each (k + 1/2) 2^-21
+    for w0, w1 in ((0, 0), (0xFFFFFFFF, 0xFFFFFFFF), (0x80000000, 1), (0x12345678, 0x9ABCDEF0)):
+        b = (w0 << 32) | w1
+        want = [(((b >> s) & 0x1FFFFF) + 0.5) / 2**21 for s in (43, 22, 1)]
+        got = O.step_uniforms([w0, w1])
+        assert got == want
+        assert all(0.0 < u < 1.0 and float(np.float32(u)) == u for u in got)
+
+
+def test_step_uniforms_distribution():
+    rng = np.random.default_rng(5)
+    w = rng.integers(0, 2**32, size=(20000, 2), dtype=np.uint64)
+    u = np.array([O.step_uniforms(O.philox2x32_10([int(a), int(b)], 7)) for a, b in w[:4000]])
+    for j in range(3):
+        assert abs(u[:, j].mean() - 0.5) < 0.015
+        assert abs(u[:, j].var() - 1 / 12) < 0.005
+    assert abs(np.corrcoef(u.T)[0, 1]) < 0.05 and abs(np.corrcoef(u.T)[1, 2]) < 0.05
+
+
 def test_uniform_open_interval_and_exact_float32():
     for w in (0, 1, 511, 512, 0x7FFFFFFF, 0xFFFFFFFF):
         u = O.uniform(w)
