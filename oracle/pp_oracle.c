@@ -15,10 +15,11 @@
  * fixed key (0x243F6A88, 0x85A308D3) with counter (seed lo, seed hi,
  * photon lo, photon hi) for a photon index below 2^40; its words w0..w2 give
  * the emission draws (wavelength, polar angle or track position, azimuth) as
- * 23-bit uniforms.  Steps: the photon's own Philox2x32-10 stream, keyed by
- * w3, with counter (the low 9 bits of w0, w1, w2 packed into 27 bits,
- * photon hi | (k + 1) << 8) for step k; its 64 output bits give three 21-bit
- * uniforms (step length, HG cos(theta), azimuth).
+ * 23-bit uniforms.  Steps: the photon's own Philox2x32-10 stream under the
+ * fixed step key 0x13198A2E, with counter (w3, base + (photon hi |
+ * (k + 1) << 8)) for step k, where base packs the low 9 bits of w0, w1, w2
+ * into 27 bits; its 64 output bits give three 21-bit uniforms (step length,
+ * HG cos(theta), azimuth).
  */
 #include "pp_oracle.h"
 
@@ -32,6 +33,7 @@
 #define ORC_C_VAC 0.299792458
 #define ORC_KEY0 0x243F6A88u /* fixed Philox key */
 #define ORC_KEY1 0x85A308D3u
+#define ORC_STEP_KEY 0x13198A2Eu /* fixed Philox2x32 key of the step blocks */
 #define ORC_TWO_PI 6.283185307179586
 
 /* Philox4x32-10, Salmon, Moraes, Dror, Shaw, "Parallel random numbers: as
@@ -83,11 +85,12 @@ void orc_step_uniforms(const uint32_t w[2], double u[3]) {
   for (int i = 0; i < 3; ++i) u[i] = ((double)((b >> (43 - 21 * i)) & 0x1FFFFFu) + 0.5) * (1.0 / 2097152.0);
 }
 
-/* The step stream of a photon from its emission block: key w3, counter word
- * 0 the low 9 bits of w0, w1 and w2. */
-void orc_step_stream(const uint32_t w[4], uint32_t* key, uint32_t* word0) {
-  *key = w[3];
-  *word0 = (w[0] & 0x1FFu) | ((w[1] & 0x1FFu) << 9) | ((w[2] & 0x1FFu) << 18);
+/* The step stream of a photon from its emission block: counter word 0 is
+ * w3, counter word 1 a base (the low 9 bits of w0, w1 and w2) plus the
+ * photon's top index bits and block number. */
+void orc_step_stream(const uint32_t w[4], uint32_t* word0, uint32_t* base) {
+  *word0 = w[3];
+  *base = (w[0] & 0x1FFu) | ((w[1] & 0x1FFu) << 9) | ((w[2] & 0x1FFu) << 18);
 }
 
 /* 23-bit uniform in the open interval (0, 1): ((w >> 9) + 1/2) * 2^-23.
@@ -193,21 +196,21 @@ static void hb_push(hitbuf* b, const orc_hit* h) {
 }
 
 /* Emission block of a photon: its three uniforms and the step stream. */
-static void emission_block(uint64_t seed, int64_t photon, double u[3], uint32_t* skey, uint32_t* sword) {
+static void emission_block(uint64_t seed, int64_t photon, double u[3], uint32_t* sc0, uint32_t* sc1) {
   uint32_t key[2] = {ORC_KEY0, ORC_KEY1};
   uint32_t ctr[4] = {(uint32_t)seed, (uint32_t)(seed >> 32), (uint32_t)(uint64_t)photon,
                      (uint32_t)((uint64_t)photon >> 32)};
   uint32_t w[4];
   orc_philox4x32_10(ctr, key, w);
   for (int i = 0; i < 3; ++i) u[i] = orc_uniform(w[i]);
-  orc_step_stream(w, skey, sword);
+  orc_step_stream(w, sc0, sc1);
 }
 
 /* Uniforms of step k of a photon. */
-static void step_block(uint32_t skey, uint32_t sword, int64_t photon, int k, double u[3]) {
-  uint32_t ctr[2] = {sword, (uint32_t)((uint64_t)photon >> 32) | ((uint32_t)(k + 1) << 8)};
+static void step_block(uint32_t sc0, uint32_t sc1, int64_t photon, int k, double u[3]) {
+  uint32_t ctr[2] = {sc0, sc1 + ((uint32_t)((uint64_t)photon >> 32) | ((uint32_t)(k + 1) << 8))};
   uint32_t w[2];
-  orc_philox2x32_10(ctr, skey, w);
+  orc_philox2x32_10(ctr, ORC_STEP_KEY, w);
   orc_step_uniforms(w, u);
 }
 
@@ -237,8 +240,8 @@ static int simulate_photon(const orc_tables* T, const orc_pair* P, int64_t pair_
                            const orc_opts* O, orc_hit* out, int64_t* steps) {
   const int compat = (O->mode == 0);
   double u[3];
-  uint32_t skey, sword;
-  emission_block(P->seed, ph, u, &skey, &sword);
+  uint32_t sc0, sc1;
+  emission_block(P->seed, ph, u, &sc0, &sc1);
   /* initialize_wavelength, src/photon_prop_cuda.jl:73-75 */
   double wl = (T->n_knots == 1) ? T->knots[0] : orc_interp_equidistant(u[0], T->knots, T->n_knots, 0.0, 1.0);
   double phi = ORC_TWO_PI * u[2]; /* uniform(0, 2pi), :54 */
@@ -282,7 +285,7 @@ static int simulate_photon(const orc_tables* T, const orc_pair* P, int64_t pair_
   double rsq = P->radius * P->radius;
   for (int k = 0; k < O->max_steps; ++k) {
     ++*steps;
-    step_block(skey, sword, ph, k, u);
+    step_block(sc0, sc1, ph, k, u);
     double step = -log(u[0]) * sca_len; /* :322-323 */
     double a = 0.0, pp = 0.0;           /* :330-337 */
     for (int j = 0; j < 3; ++j) {

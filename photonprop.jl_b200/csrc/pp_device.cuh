@@ -97,10 +97,10 @@ __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c[4], uint32_t k
   }
 }
 
-// Philox2x32-10 (same paper): one multiplier and one key word, whose Weyl
-// increments are added per round (the key varies per photon).  A block gives
+// Philox2x32-10 (same paper): one multiplier and one key word.  A block gives
 // 64 bits for two 32x32 products per round, against 128 bits for four in a
-// Philox4x32 block; a step needs 63 bits.
+// Philox4x32 block; a step needs 63 bits.  Under a fixed key (the steps') the
+// round keys are immediates.
 __host__ __device__ __forceinline__ void philox2x32_10(uint32_t& c0, uint32_t& c1, uint32_t k) {
 #pragma unroll
   for (int r = 0; r < 10; ++r) {
@@ -130,8 +130,9 @@ __device__ __forceinline__ float u01(uint32_t w) {
   return __uint_as_float(m) - __uint_as_float(0x3F7FFFFFu);
 }
 
-constexpr uint32_t kKey0 = 0x243F6A88u;  // fixed Philox key (hex digits of pi)
+constexpr uint32_t kKey0 = 0x243F6A88u;  // fixed Philox4x32 key of the emission blocks (hex digits of pi)
 constexpr uint32_t kKey1 = 0x85A308D3u;
+constexpr uint32_t kStepKey = 0x13198A2Eu;  // fixed Philox2x32 key of the step blocks (the digits that follow)
 
 // Photon index bits 32..39 and a step's block number (step k: k + 1) above
 // them: word 3 of the emission counter (block 0) and word 1 of the step
@@ -142,27 +143,31 @@ __device__ __forceinline__ uint32_t ctr_word(uint64_t photon, uint32_t block) {
 
 // Emission block of a photon: Philox4x32-10 under the fixed key with counter
 // (seed lo, seed hi, photon lo, photon hi).  Words 0..2 give the emission's
-// uniforms (their top 23 bits), word 3 and the low 9 bits of words 0..2 the
-// key and counter word 0 of the photon's step stream.
+// uniforms (their top 23 bits); word 3 and the low 9 bits of words 0..2 name
+// the photon's step stream: step k is the Philox2x32-10 block under the
+// fixed step key at counter (word 3, base + ctr_word(photon, k + 1)), where
+// base packs those 27 low bits.
 __device__ __forceinline__ uint4 emission_block(uint32_t seed_lo, uint32_t seed_hi, uint64_t photon) {
   uint32_t c[4] = {seed_lo, seed_hi, (uint32_t)photon, ctr_word(photon, 0u)};
   philox4x32_10(c, kKey0, kKey1);
   return make_uint4(c[0], c[1], c[2], c[3]);
 }
 __device__ __forceinline__ Draw3 emission_uniforms(const uint4& w) { return Draw3{u01(w.x), u01(w.y), u01(w.z)}; }
-__device__ __forceinline__ uint32_t step_word0(const uint4& w) {
+__device__ __forceinline__ uint32_t step_base(const uint4& w) {
   return (w.x & 0x1FFu) | ((w.y & 0x1FFu) << 9) | ((w.z & 0x1FFu) << 18);
 }
 
 // A step's three uniforms from its Philox2x32 block (w0, w1): bits 63..43,
 // 42..22 and 21..1 of w0:w1, each placed in mantissa bits 22..2 of 1.m with
 // bit 1 set, so that 1.m - 1 = (k + 1/2) 2^-21 exactly.
+// The first and third fields are shifted into place by integer multiply-adds
+// (FMA pipe) rather than shifts (the half-rate ALU pipe): the same bits.
 __device__ __forceinline__ Draw3 step_uniforms(uint32_t w0, uint32_t w1) {
-  const uint32_t m0 = (w0 >> 9) & 0x7FFFFCu;
+  uint32_t b0, b2;
+  asm("mad.hi.u32 %0, %1, %2, %3;" : "=r"(b0) : "r"(w0 & 0xFFFFF800u), "r"(1u << 23), "r"(0x3F800002u));
+  asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(b2) : "r"(w1 & 0x003FFFFEu), "r"(2u), "r"(0x3F800002u));
   const uint32_t m1 = __funnelshift_r(w1, w0, 20) & 0x7FFFFCu;
-  const uint32_t m2 = (w1 << 1) & 0x7FFFFCu;
-  return Draw3{__uint_as_float(m0 | 0x3F800002u) - 1.f, __uint_as_float(m1 | 0x3F800002u) - 1.f,
-               __uint_as_float(m2 | 0x3F800002u) - 1.f};
+  return Draw3{__uint_as_float(b0) - 1.f, __uint_as_float(m1 | 0x3F800002u) - 1.f, __uint_as_float(b2) - 1.f};
 }
 
 // ---- resident tables (one copy per context, staged into shared memory) ----
@@ -328,10 +333,21 @@ struct Photon {
   float path;         // physical: path left before t_max; compat: path travelled
   float neg_ln2_len;  // -ln2 * scattering length: step = lg2(u) * this
   uint32_t ctr3;      // Philox counter word of the next event: block (= steps + 1) << 8 | photon bits 32..39
-  uint32_t skey;      // the step stream's Philox2x32 key and counter word 0 (from the emission block)
-  uint32_t sword;
-  uint64_t id;
+  uint32_t sc0;       // the step stream (from the emission block): counter word 0
+  uint32_t sc1;       // and the base added to ctr3 for counter word 1
+  uint32_t id_lo;     // photon index bits 0..31 (bits 32..39 are the low byte of ctr3)
 };
+
+// The photon's index: bits 0..31 in id_lo, 32..39 in the low byte of ctr3
+// (which keeps them for every block), so the index costs one register.
+__device__ __forceinline__ uint64_t photon_index(const Photon& s) {
+  return ((uint64_t)(s.ctr3 & 0xFFu) << 32) | s.id_lo;
+}
+// Sets the photon's index with its counter at block 0 (emission pending).
+__device__ __forceinline__ void set_photon(Photon& s, uint64_t id) {
+  s.id_lo = (uint32_t)id;
+  s.ctr3 = ctr_word(id, 0u);
+}
 
 struct PairCtx {
   float r;  // sphere radius
@@ -457,13 +473,14 @@ __device__ __forceinline__ float path_at_tmax(const DevTables& T, const RunParam
   return (R.t_max - f.t_emit) * kCVac * rcp(group_index(T, rcp(f.wl)));
 }
 
-// Emission of photon s.id (its emission block): position, direction, the
+// Emission of photon photon_index(s) (its emission block): position, direction, the
 // per-wavelength constants and the step stream; afterwards the next event
 // is step 0 (step block 1).
 template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                            const PairCtx& c, Photon& s) {
-  const uint4 w = emission_block(c.seed_lo, c.seed_hi, s.id);
+  const uint64_t id = photon_index(s);
+  const uint4 w = emission_block(c.seed_lo, c.seed_hi, id);
   const Draw3 d = emission_uniforms(w);
   const EmissionFrame f = emission_frame<MODE, EM>(T, P, d);
   const float3 tg = pair_target(P);
@@ -473,9 +490,9 @@ __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& 
   s.path = (MODE == kPhysical) ? path_at_tmax(T, R, f) : 0.f;
   s.neg_ln2_len = -kLn2 * scattering_length(T, f.wl);
   emission_direction(f, d.u2, s.dx, s.dy, s.dz);
-  s.skey = w.w;
-  s.sword = step_word0(w);
-  s.ctr3 = ctr_word(s.id, 1u);
+  s.sc0 = w.w;
+  s.sc1 = step_base(w);
+  s.ctr3 = ctr_word(id, 1u);
 }
 
 // Step k (block k + 1 of the photon's Philox2x32 stream) of
@@ -485,8 +502,8 @@ __device__ __forceinline__ void emit_event(const DevTables& T, const RunParams& 
 // length then at the hit).
 template <int MODE>
 __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c, Photon& s, bool& hit) {
-  uint32_t w0 = s.sword, w1 = s.ctr3;
-  philox2x32_10(w0, w1, s.skey);
+  uint32_t w0 = s.sc0, w1 = s.sc1 + s.ctr3;
+  philox2x32_10(w0, w1, kStepKey);
   const Draw3 d = step_uniforms(w0, w1);
   const float step = lg2(d.u0) * s.neg_ln2_len;
   const float ex = s.px, ey = s.py, ez = s.pz;  // photon - sphere centre
@@ -556,7 +573,7 @@ struct HitValues {
 template <int MODE, int EM = kEmBasic>
 __device__ __forceinline__ HitValues hit_values(const DevTables& T, const RunParams& R, const pp_pair* __restrict__ P,
                                                 const PairCtx& c, const Photon& s) {
-  const Draw3 d = emission_uniforms(emission_block(c.seed_lo, c.seed_hi, s.id));
+  const Draw3 d = emission_uniforms(emission_block(c.seed_lo, c.seed_hi, photon_index(s)));
   const EmissionFrame f = emission_frame<MODE, EM>(T, P, d);
   HitValues h;
   h.wl = f.wl;
@@ -595,7 +612,7 @@ __device__ __forceinline__ void write_hit(const RunParams& R, const PairCtx& c, 
     if (R.flags & PP_OPT_COMPACT_HITS) {
       float4* dst = reinterpret_cast<float4*>(reinterpret_cast<pp_hit32*>(R.hits) + idx);
       dst[0] = make_float4(h.px, h.py, h.pz, h.time);
-      dst[1] = make_float4(h.weight, h.wl, __uint_as_float((uint32_t)s.id),
+      dst[1] = make_float4(h.weight, h.wl, __uint_as_float(s.id_lo),
                            __uint_as_float((uint32_t)c.index + R.pair_base));
     } else {
       float4* dst = reinterpret_cast<float4*>(R.hits + idx);
@@ -603,7 +620,7 @@ __device__ __forceinline__ void write_hit(const RunParams& R, const PairCtx& c, 
       dst[1] = make_float4(h.d0x, h.d0y, h.d0z, h.weight);
       dst[2] = make_float4(s.dx, s.dy, s.dz, h.wl);
       dst[3] = make_float4(h.dist, __uint_as_float((uint32_t)c.index + R.pair_base),
-                           __uint_as_float((uint32_t)s.id), __uint_as_float((uint32_t)(s.id >> 32)));
+                           __uint_as_float(s.id_lo), __uint_as_float(s.ctr3 & 0xFFu));
     }
   } else {
     atomicOr(R.counters + 2, 1ull);

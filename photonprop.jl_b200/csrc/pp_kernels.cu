@@ -37,7 +37,7 @@ struct __align__(16) Staged {
   uint32_t id_lo, id_hi;
   int32_t pair;
   float radius;         // the pair's sphere radius, so that a refill reads
-  uint32_t skey, sword;  // shared memory only, and the photon's step stream
+  uint32_t sc0, sc1;  // shared memory only, and the photon's step stream
   uint32_t pad[2];
 };
 
@@ -48,6 +48,16 @@ struct __align__(16) Staged {
 // staged hits together, converged, instead of one or two lanes walking the
 // hit path while the others wait.
 constexpr unsigned kHitStage = 32;
+
+// A warp's current photon chunk (warp-uniform): kept in shared memory, since
+// only the warp's emission pass reads or advances it, so that the step loop
+// holds no registers for it.
+struct WarpChunk {
+  unsigned long long base;  // first photon index of the chunk
+  unsigned next, len;
+  int pair;
+  int done;  // the work queue is exhausted
+};
 struct StagedHit {
   float px, py, pz, dx, dy, dz, path;
   uint32_t id_lo, id_hi;
@@ -65,11 +75,17 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
   __shared__ Staged stage[WARPS][kStage];
   __shared__ WarpStats wstats[WARPS];
   __shared__ StagedHit hstage[MODE == kCompat ? WARPS : 1][kHitStage];
+  __shared__ WarpChunk wchunk[WARPS];
   stage_tables(T, R.tables);
   if ((threadIdx.x & 31u) == 0) {
     WarpStats& w0 = wstats[threadIdx.x >> 5];
     w0.pair = -1;
     for (int k = 0; k < 6; ++k) w0.v[k] = 0.0;
+    WarpChunk& q = wchunk[threadIdx.x >> 5];
+    q.base = 0;
+    q.next = q.len = 0;
+    q.pair = 0;
+    q.done = 0;
   }
   __syncthreads();
 
@@ -93,9 +109,9 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
       p.dz = g.dz;
       p.path = g.path;
       p.neg_ln2_len = 0.f;
-      p.id = ((unsigned long long)g.id_hi << 32) | g.id_lo;
-      p.ctr3 = 0u;
-      p.skey = p.sword = 0u;
+      p.id_lo = g.id_lo;
+      p.ctr3 = g.id_hi;  // block 0: the index's top bits only
+      p.sc0 = p.sc1 = 0u;
       const PairCtx pc = load_pair_ctx(R.pairs + g.pair, g.pair);
       const HitValues h = hit_values<MODE, EM>(T, R, R.pairs + g.pair, pc, p);
       record_hit_cached(R, ws, pc, p, h);
@@ -103,19 +119,16 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
     __syncwarp();
   };
 
-  // warp-uniform state: the current chunk and the ring
-  unsigned long long c_base = 0;  // first photon index of the chunk
-  unsigned c_next = 0, c_len = 0;
-  int c_pair = 0;
-  bool queue_done = false;
+  // warp-uniform state: the ring (the current chunk is in shared memory)
+  WarpChunk* wq = &wchunk[threadIdx.x >> 5];
   unsigned r_head = 0, r_count = 0;
 
   // lane state
   bool alive = false;
   Photon s;
-  s.id = 0;
+  s.id_lo = 0;
   s.ctr3 = 1u << 8;
-  s.skey = s.sword = 0u;
+  s.sc0 = s.sc1 = 0u;
   s.px = s.py = s.pz = s.dx = s.dy = s.path = s.neg_ln2_len = 0.f;
   s.dz = 1.f;
   // the lane's pair: radius and index (the seed, which only a hit's emission
@@ -129,7 +142,11 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
   for (;;) {
     const unsigned need = __ballot_sync(kFull, !alive);
     const unsigned n_need = __popc(need);
-    if (r_count < n_need && !queue_done) {
+    if (r_count < n_need && !wq->done) {
+      unsigned long long c_base = wq->base;
+      unsigned c_next = wq->next, c_len = wq->len;
+      int c_pair = wq->pair;
+      bool queue_done = false;
       // give every lane the next photon index of the queue
       bool have = false;
       unsigned long long pid = 0;
@@ -180,18 +197,25 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         c_next += take;
         filled += take;
       }
+      if (lane == 0) {
+        wq->base = c_base;
+        wq->next = c_next;
+        wq->len = c_len;
+        wq->pair = c_pair;
+        wq->done = queue_done;
+      }
       if (have) {
         const pp_pair* P = R.pairs + ppair;
         const PairCtx pc = load_pair_ctx(P, ppair);
         Photon e;
-        e.id = pid;
+        set_photon(e, pid);
         emit_event<MODE, EM>(T, R, P, pc, e);
         float4* dst = reinterpret_cast<float4*>(ring + ((r_head + r_count + lane) & (kStage - 1)));
         dst[0] = make_float4(e.px, e.py, e.pz, e.dx);
         dst[1] = make_float4(e.dy, e.dz, e.neg_ln2_len, e.path);
         dst[2] = make_float4(__uint_as_float((uint32_t)pid), __uint_as_float((uint32_t)(pid >> 32)),
                              __int_as_float(ppair), pc.r);
-        dst[3] = make_float4(__uint_as_float(e.skey), __uint_as_float(e.sword), 0.f, 0.f);
+        dst[3] = make_float4(__uint_as_float(e.sc0), __uint_as_float(e.sc1), 0.f, 0.f);
       }
       r_count += filled;
       __syncwarp();
@@ -209,12 +233,12 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
         s.dz = b.y;
         s.neg_ln2_len = b.z;
         s.path = b.w;
-        s.id = ((unsigned long long)__float_as_uint(d.y) << 32) | __float_as_uint(d.x);
-        s.ctr3 = ctr_word(s.id, 1u);
+        s.id_lo = __float_as_uint(d.x);
+        s.ctr3 = __float_as_uint(d.y) | (1u << 8);  // index bits 32..39, step 0
         c.index = __float_as_int(d.z);
         c.r = d.w;
-        s.skey = __float_as_uint(e.x);
-        s.sword = __float_as_uint(e.y);
+        s.sc0 = __float_as_uint(e.x);
+        s.sc1 = __float_as_uint(e.y);
         alive = true;
       }
     }
@@ -245,8 +269,8 @@ __global__ void __launch_bounds__(WARPS * 32, (EM == kEmCascade ? 768 : 1024) / 
           g.dy = s.dy;
           g.dz = s.dz;
           g.path = s.path;
-          g.id_lo = (uint32_t)s.id;
-          g.id_hi = (uint32_t)(s.id >> 32);
+          g.id_lo = s.id_lo;
+          g.id_hi = s.ctr3 & 0xFFu;
           g.pair = c.index;
         }
         h_count += nh;
@@ -289,8 +313,7 @@ __global__ void __launch_bounds__(512) plain_kernel(const RunParams R, const pp_
   for (unsigned long long id = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; id < n;
        id += stride) {
     Photon s;
-    s.id = id;
-    s.ctr3 = ctr_word(id, 0u);
+    set_photon(s, id);
     s.dx = s.dy = 0.f;
     s.dz = 1.f;
     bool alive = true;
@@ -335,8 +358,7 @@ __global__ void __launch_bounds__(1024) stacks_kernel(const RunParams R, const p
   for (long long i = 0; i < per_thread; ++i) {
     if (*(volatile int*)&cursor > ix_offset + stack_len - safe_margin) break;
     Photon s;
-    s.id = g + (unsigned long long)i * G;
-    s.ctr3 = ctr_word(s.id, 0u);
+    set_photon(s, g + (unsigned long long)i * G);
     s.dx = s.dy = 0.f;
     s.dz = 1.f;
     bool alive = true;
@@ -566,9 +588,10 @@ __global__ void __launch_bounds__(256, 4) peak_step_kernel(const RunParams R, in
   c.seed_lo = c.seed_hi = 0u;
   c.index = 0;
   Photon s;
-  s.skey = 0x9E3779B9u * (blockIdx.x + 1u);
-  s.sword = 0x2545F491u ^ threadIdx.x;
-  s.id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  s.sc0 = 0x9E3779B9u * (blockIdx.x + 1u) ^ threadIdx.x;
+  s.sc1 = 0x2545F491u & 0x7FFFFFFu;
+  const uint64_t id = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  s.id_lo = (uint32_t)id;
   s.px = 100.f + (float)(threadIdx.x & 31u);
   s.py = 50.f;
   s.pz = -30.f;
@@ -577,7 +600,7 @@ __global__ void __launch_bounds__(256, 4) peak_step_kernel(const RunParams R, in
   s.dz = 0.8f;
   s.path = 1e30f;
   s.neg_ln2_len = -kLn2 * 30.f;
-  s.ctr3 = ctr_word(s.id, 1u);
+  s.ctr3 = ctr_word(id, 1u);
   unsigned live = 0;
   for (int i = 0; i < iters; ++i) {
     bool hit = false;
