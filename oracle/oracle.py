@@ -77,6 +77,7 @@ def lib():
         L.orc_philox4x32_10.argtypes = [u32p, u32p, u32p]
         L.orc_philox2x32_10.argtypes = [u32p, ctypes.c_uint32, u32p]
         L.orc_step_uniforms.argtypes = [u32p, ctypes.POINTER(ctypes.c_double)]
+        L.orc_scatter_turn.argtypes = [dp, dp, dp]
         L.orc_uniform.argtypes = [ctypes.c_uint32]
         L.orc_uniform.restype = ctypes.c_double
         L.orc_hg_costheta.argtypes = [ctypes.c_double, ctypes.c_double]
@@ -128,6 +129,15 @@ def step_uniforms(w):
     u = (ctypes.c_double * 3)()
     lib().orc_step_uniforms(c, u)
     return list(u)
+
+
+def scatter_turn(old, new):
+    """Physical-mode scattering turn of direction `old` by the local vector `new`."""
+    o = np.ascontiguousarray(old, dtype=np.float64)
+    n = np.ascontiguousarray(new, dtype=np.float64)
+    out = np.zeros(3)
+    lib().orc_scatter_turn(_dptr(o), _dptr(n), _dptr(out))
+    return out
 
 
 def uniform(w):

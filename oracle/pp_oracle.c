@@ -9,6 +9,8 @@
  *   - Cherenkov-cone emission: a point uniform along the track, emission angle
  *     acos(1/n(lambda)) around the track axis, emission time t0 + s/c;
  *   - arrival time t = t_emit + dist * n_group(lambda) / c;
+ *   - a scattering turns the direction in the frame of its meridian
+ *     (orc_scatter_turn; the reference's rotate_to_axis frame in compat mode);
  *   - a photon ends when its next position would lie beyond the time window
  *     t_max, when it hits the sphere, or after max_steps steps.
  * Random numbers (Salmon et al., SC'11).  Emission: Philox4x32-10 under the
@@ -130,6 +132,24 @@ void orc_rotate_to_axis(const double o[3], const double n[3], double out[3]) {
   out[0] = x * r;
   out[1] = y * r;
   out[2] = z * r;
+}
+
+/* Physical-mode scattering turn (no reference code: the reference turns with
+ * rotate_to_axis in both modes): the local vector n = (a, b, c) placed in
+ * the frame whose first axis is the old direction u's meridian,
+ *   x = (ux uz a - uy b) / s + ux c, y = (uy uz a + ux b) / s + uy c,
+ *   z = -a s + uz c, s = sqrt(ux^2 + uy^2).
+ * The azimuth is uniform, so this is the same scattering distribution as the
+ * Rodrigues frame; the CUDA kernels use this frame in physical mode. */
+void orc_scatter_turn(const double u[3], const double n[3], double out[3]) {
+  const double s2 = u[0] * u[0] + u[1] * u[1];
+  const double rs = 1.0 / sqrt(s2);
+  const double p = u[2] * n[0];
+  const double X = u[0] * p - u[1] * n[1];
+  const double Y = u[1] * p + u[0] * n[1];
+  out[0] = X * rs + u[0] * n[2];
+  out[1] = Y * rs + u[1] * n[2];
+  out[2] = -n[0] * s2 * rs + u[2] * n[2];
 }
 
 /* update_position, src/photon_prop_cuda.jl:255-259. */
@@ -341,7 +361,10 @@ static int simulate_photon(const orc_tables* T, const orc_pair* P, int64_t pair_
     double ph2 = ORC_TWO_PI * u[2];
     double loc[3] = {cos(ph2) * ss, sin(ph2) * ss, cs};
     double nd[3];
-    orc_rotate_to_axis(dir, loc, nd);
+    if (compat)
+      orc_rotate_to_axis(dir, loc, nd);
+    else
+      orc_scatter_turn(dir, loc, nd);
     dir[0] = nd[0];
     dir[1] = nd[1];
     dir[2] = nd[2];

@@ -84,6 +84,7 @@ typedef struct {
 void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
 void orc_philox2x32_10(const uint32_t ctr[2], uint32_t key, uint32_t out[2]);
 void orc_step_uniforms(const uint32_t w[2], double u[3]);
+void orc_scatter_turn(const double u[3], const double n[3], double out[3]);
 void orc_step_stream(const uint32_t w[4], uint32_t* word0, uint32_t* base);
 double orc_uniform(uint32_t w);
 double orc_hg_costheta(double g, double u);

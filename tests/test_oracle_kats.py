@@ -54,6 +54,27 @@ def test_step_uniforms_distribution():
     assert abs(np.corrcoef(u.T)[0, 1]) < 0.05 and abs(np.corrcoef(u.T)[1, 2]) < 0.05
 
 
+def test_scatter_turn_frame():
+    # physical-mode turn: unit output at polar angle acos(c) from the old
+    # direction, and the same turn as rotate_to_axis up to an azimuth
+    rng = np.random.default_rng(9)
+    for _ in range(200):
+        u = rng.normal(size=3)
+        u /= np.linalg.norm(u)
+        c = rng.uniform(-1, 1)
+        phi = rng.uniform(0, 2 * np.pi)
+        n = np.array([np.cos(phi) * np.sqrt(1 - c * c), np.sin(phi) * np.sqrt(1 - c * c), c])
+        r = O.scatter_turn(u, n)
+        assert abs(np.linalg.norm(r) - 1) < 1e-12
+        assert abs(r @ u - c) < 1e-12
+        r2 = O.rotate_to_axis(u, n)
+        assert abs(r2 @ u - c) < 1e-12
+    # the frame's first axis is the meridian: azimuth 0 tilts toward -z for an upward direction
+    u = np.array([0.6, 0.0, 0.8])
+    r = O.scatter_turn(u, [1.0, 0.0, 0.0])
+    np.testing.assert_allclose(r, [0.8, 0.0, -0.6], atol=1e-12)
+
+
 def test_uniform_open_interval_and_exact_float32():
     for w in (0, 1, 511, 512, 0x7FFFFFFF, 0xFFFFFFFF):
         u = O.uniform(w)
