@@ -1114,7 +1114,7 @@ def run_ours(args):
                      "peak_source": "measured live: ex2.approx dependent chains over every SM (pp_measure_peaks)",
                      "counts": "achieved = algorithmic MUFU operations (the reference's arithmetic: 7 per photon "
                                "step, 10 per isotropic / 14 per cone photon start) per second; 'issued' = this "
-                               "kernel's own count (7 MUFU and 56 FP32 per step, ncu opcode counts)",
+                               "kernel's own count (7 MUFU and 46 FP32 per step, ncu opcode counts)",
                      "issued": {"mufu_achieved": mufu_i / t_local / 1e9,
                                 "mufu_frac": mufu_i / t_local / peaks["mufu_ops"],
                                 "fp32_frac": fp32_i / t_local / peaks["fp32_ops"]},

@@ -8,12 +8,14 @@ per photon step   7 MUFU  the reference's arithmetic (src/photon_prop_cuda.jl:
                           square root of the ray-sphere discriminant when the
                           line meets the sphere; the roofline counts 7.  This
                           kernel issues 7 as well (lg2, sqrt of the
-                          discriminant, rcp, sqrt, sin, cos, rcp: the rotation
-                          needs no sin(theta) and renormalises with a Newton
-                          step), which ncu's opcode counts of the bare-step
-                          kernel confirm.
-                 ~45 FP32 in the reference's form; this kernel issues 56
-                          (ncu: 28 FFMA, 20 FMUL, 8 FADD per step).
+                          discriminant, rcp, sqrt, sin, cos and the turn's
+                          rsqrt in physical mode, rcp in the compat-mode
+                          rotation), which ncu's opcode counts of the
+                          bare-step kernel confirm.
+                 ~45 FP32 in the reference's form; this kernel issues 46
+                          (ncu: 24 FFMA, 17 FMUL, 5 FADD per step; the
+                          physical-mode turn in the meridian frame, without
+                          renormalisation).
                   1 Philox2x32-10 block (20 32x32-bit products: half a
                           Philox4x32-10 block, as which it is counted).
 per photon start  isotropic: 10 MUFU, 28 FP32; Cherenkov cone: 14 MUFU, 60 FP32;
@@ -24,7 +26,7 @@ A photon that hits the sphere also re-draws its emission block (rare).
 MUFU_PER_STEP_ALG = 7
 FP32_PER_STEP_ALG = 45
 MUFU_PER_STEP = 7
-FP32_PER_STEP = 56
+FP32_PER_STEP = 46
 PHILOX_PER_STEP = 0.5  # Philox4x32-10 block equivalents (by 32x32-bit products)
 MUFU_PER_PHOTON = {0: 10, 1: 14}   # by emitter type
 FP32_PER_PHOTON = {0: 28, 1: 60}
@@ -51,6 +53,6 @@ def op_counts(steps, photons_iso, photons_cone, algorithmic=False):
 # stays in the 126 MB L2 during the launch and reaches DRAM afterwards.
 NCU_DRAM_BYTES_PER_LAUNCH = 0.5 * ((2.43 + 25.48) + (3.35 + 34.66)) * 1e6
 # Issue and pipes on one launch of 512 mixed pairs (<= 1e6 photons each).
-NCU_ISSUE_ACTIVE = 0.778
-NCU_PIPES = {"alu": 0.487, "fma": 0.347, "xu": 0.322}  # pipe utilisation, same capture
-NCU_LANES_ACTIVE = 30.0  # threads per executed warp instruction, same capture
+NCU_ISSUE_ACTIVE = 0.780
+NCU_PIPES = {"alu": 0.494, "fma": 0.390, "xu": 0.375}  # pipe utilisation, same capture
+NCU_LANES_ACTIVE = 29.97  # threads per executed warp instruction, same capture
