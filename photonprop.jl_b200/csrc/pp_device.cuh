@@ -474,14 +474,17 @@ __device__ __forceinline__ float sin_from_cos(float c) { return sqrt_a(fmaxf(0.f
 __device__ __forceinline__ void scatter_turn(float ux, float uy, float uz, float cpol, float spol, float u,
                                              float& rx, float& ry, float& rz) {
   const float ph = fmaf(kTwoPi, u, -kPi);
-  const float a = -cos_a(ph) * spol, b = -sin_a(ph) * spol;
+  const float2 ab = __fmul2_rn(make_float2(-cos_a(ph), -sin_a(ph)), make_float2(spol, spol));
+  const float a = ab.x, b = ab.y;
   const float s2 = fmaf(ux, ux, uy * uy);
   const float rs = rsqrt_a(s2);
   const float p = uz * a;
   const float X = fmaf(ux, p, -uy * b);
   const float Y = fmaf(uy, p, ux * b);
-  rx = fmaf(X, rs, ux * cpol);
-  ry = fmaf(Y, rs, uy * cpol);
+  const float2 rxy = __ffma2_rn(make_float2(X, Y), make_float2(rs, rs),
+                                __fmul2_rn(make_float2(ux, uy), make_float2(cpol, cpol)));
+  rx = rxy.x;
+  ry = rxy.y;
   rz = fmaf(-a, s2 * rs, uz * cpol);
 }
 
@@ -545,7 +548,10 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
   // b = a^2 - |e|^2 + r^2 (src/photon_prop_cuda.jl:340) evaluated as r^2 - |e - a d|^2:
   // the same number, but without cancelling two large squares, which in FP32
   // costs millimetres at grazing incidence on a sphere tens of metres away
-  const float qx = fmaf(-a, s.dx, ex), qy = fmaf(-a, s.dy, ey), qz = fmaf(-a, s.dz, ez);
+  // (x, y) pairs on sm_100's packed FP32 instructions (round to nearest: the
+  // scalar results bit for bit, in half the issue slots)
+  const float2 qxy = __ffma2_rn(make_float2(-a, -a), make_float2(s.dx, s.dy), make_float2(ex, ey));
+  const float qx = qxy.x, qy = qxy.y, qz = fmaf(-a, s.dz, ez);
   const float q = fmaf(qz, qz, fmaf(qy, qy, qx * qx));
   const float b = fmaf(c.r, c.r, -q);
   const float pp = fmaf(a, a, q);  // |e|^2
@@ -570,8 +576,9 @@ __device__ __forceinline__ bool step_event(const RunParams& R, const PairCtx& c,
     alive = move;
   }
   const float len = hit ? dd : (move ? step : 0.f);
-  s.px = fmaf(len, s.dx, s.px);
-  s.py = fmaf(len, s.dy, s.py);
+  const float2 pxy = __ffma2_rn(make_float2(len, len), make_float2(s.dx, s.dy), make_float2(s.px, s.py));
+  s.px = pxy.x;
+  s.py = pxy.y;
   s.pz = fmaf(len, s.dz, s.pz);
   s.path += (MODE == kPhysical) ? -len : len;
   const float cpol = hg_costheta(R.hg, d.u1);
