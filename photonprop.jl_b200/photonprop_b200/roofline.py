@@ -48,10 +48,10 @@ def op_counts(steps, photons_iso, photons_cone, algorithmic=False):
 # DRAM traffic of one launch of the 4096-pair benchmark batch (5.75e9
 # photons), full size, `--metrics dram__bytes_read.sum,dram__bytes_write.sum
 # --cache-control none` (one pass): the two timed launches after an L2 flush
-# read 2.4 and 3.4 MB and wrote 25.5 and 34.7 MB.  The rest of a step's
+# read 2.3 and 3.0 MB and wrote 23.1 and 32.8 MB.  The rest of a step's
 # algorithmic bytes (zeroed and accumulated FP64 histograms, hit records)
 # stays in the 126 MB L2 during the launch and reaches DRAM afterwards.
-NCU_DRAM_BYTES_PER_LAUNCH = 0.5 * ((2.43 + 25.48) + (3.35 + 34.66)) * 1e6
+NCU_DRAM_BYTES_PER_LAUNCH = 0.5 * ((2.27 + 23.11) + (3.04 + 32.76)) * 1e6
 # Issue and pipes on one launch of 512 mixed pairs (<= 1e6 photons each).
 NCU_ISSUE_ACTIVE = 0.780
 NCU_PIPES = {"alu": 0.494, "fma": 0.390, "xu": 0.375}  # pipe utilisation, same capture
