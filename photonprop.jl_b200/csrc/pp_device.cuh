@@ -266,10 +266,12 @@ struct HG {
   float two_g, one_m_g, a, one_p_g2, inv_2g;
   int iso;
 };
+// g == 0 (isotropic, where the formula divides by zero) is a select rather
+// than a branch: the formula then gives 0 (inv_2g is 0), which is dropped.
 __device__ __forceinline__ float hg_costheta(const HG& h, float u) {
-  if (h.iso) return fmaf(2.f, u, -1.f);
   const float t = h.a * rcp(fmaf(h.two_g, u, h.one_m_g));
-  return fmaf(-t, t, h.one_p_g2) * h.inv_2g;
+  const float c = fmaf(-t, t, h.one_p_g2) * h.inv_2g;
+  return h.iso ? fmaf(2.f, u, -1.f) : c;
 }
 
 // Rotation that takes e_z to the unit vector o, applied to n (the Rodrigues
