@@ -343,6 +343,7 @@ __global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, co
   }
   if (t < OUT) b4[t] = P.p[OFF_B4 + t];
   if (t < 18) nrm[t] = P.norm[t];
+  if (t < IN) nrm[18 + t] = 1.f / P.norm[4 + t];  // feature scales as reciprocals: no division per row
   if (t < kGroups) mbar_init(smem_u32(mbars + t));
   if ((t >> 5) == 0) {  // all 512 columns: 128 per group
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(smem_u32(tslot)));
@@ -377,7 +378,7 @@ __global__ void __launch_bounds__(INFER_THREADS, 1) infer_kernel(DevParams P, co
     for (int j = 0; j < IN; ++j) {
       const float raw = xr[j];
       if (j == 2) lnN = raw * 2.302585092994046f;
-      xn[j] = (raw - nrm[j]) / nrm[4 + j];
+      xn[j] = (raw - nrm[j]) * nrm[18 + j];
     }
     {
       const int64_t nrow = row + tile_step * TILE;
