@@ -38,8 +38,11 @@ def per_photon_errors(g, o):
     dw = np.abs(g["weight"].astype(np.float64) - o["weight"]) / np.maximum(o["weight"], 1e-30)
     dwl = np.abs(g["wavelength"].astype(np.float64) - o["wavelength"]) / o["wavelength"]
     dd0 = np.linalg.norm(g["dir0"].astype(np.float64) - o["dir0"], axis=1)
+    ddir = np.linalg.norm(g["dir"].astype(np.float64) - o["dir"], axis=1)
+    dnorm = np.abs(np.linalg.norm(g["dir"].astype(np.float64), axis=1) - 1.0)
     ddist = np.abs(g["dist"].astype(np.float64) - o["dist"])
-    return {"pos": dpos, "time": dt, "weight": dw, "wavelength": dwl, "dir0": dd0, "dist": ddist}
+    return {"pos": dpos, "time": dt, "weight": dw, "wavelength": dwl, "dir0": dd0, "dir": ddir, "dir_norm": dnorm,
+            "dist": ddist}
 
 
 def summary(err):
@@ -77,9 +80,11 @@ def chi2_two_sample(a, b, min_count=10):
 def check_matched(g, o, n_gpu_only, n_orc_only, label, flip_frac=0.01, flip_abs=3):
     """Per-photon tolerances of matched hits (GPU FP32 against the FP64 oracle
     on the same Philox numbers):  |d pos| <= 2e-3 m + 2e-5 path,
-    |d t| <= 1e-2 ns + 1e-5 t, |d w| <= 1e-3 w + 1e-8, |d lambda| / lambda <= 1e-5;
-    photons detected on one side only (sphere-rim flips) <= flip_frac of the
-    hits + flip_abs."""
+    |d t| <= 1e-2 ns + 1e-5 t, |d w| <= 1e-3 w + 1e-8, |d lambda| / lambda <= 1e-5,
+    arrival direction |d dir| <= 1e-3 with | |dir| - 1 | <= 1e-5 (the
+    physical-mode turn is not renormalised: its norm error must stay
+    bounded); photons detected on one side only (sphere-rim flips) <=
+    flip_frac of the hits + flip_abs."""
     err = per_photon_errors(g, o)
     s = summary(err)
     print(label, "matched", len(g), "gpu-only", n_gpu_only, "oracle-only", n_orc_only, s)
@@ -91,6 +96,8 @@ def check_matched(g, o, n_gpu_only, n_orc_only, label, flip_frac=0.01, flip_abs=
     # relative 1e-3, plus an absolute floor where the PMT acceptance tends to zero
     assert np.all(np.abs(g["weight"] - o["weight"]) <= 1e-3 * o["weight"] + 1e-8), (label, s["weight"])
     assert np.all(err["wavelength"] <= 1e-5), (label, s["wavelength"])
+    assert np.all(err["dir"] <= 1e-3), (label, s["dir"])
+    assert np.all(err["dir_norm"] <= 1e-5), (label, s["dir_norm"])
     return s
 
 
