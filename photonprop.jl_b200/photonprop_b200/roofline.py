@@ -53,6 +53,6 @@ def op_counts(steps, photons_iso, photons_cone, algorithmic=False):
 # stays in the 126 MB L2 during the launch and reaches DRAM afterwards.
 NCU_DRAM_BYTES_PER_LAUNCH = 0.5 * ((2.27 + 23.11) + (3.04 + 32.76)) * 1e6
 # Issue and pipes on one launch of 512 mixed pairs (<= 1e6 photons each).
-NCU_ISSUE_ACTIVE = 0.780
-NCU_PIPES = {"alu": 0.494, "fma": 0.390, "xu": 0.375}  # pipe utilisation, same capture
+NCU_ISSUE_ACTIVE = 0.779
+NCU_PIPES = {"alu": 0.518, "fma": 0.395, "xu": 0.375}  # pipe utilisation, same capture
 NCU_LANES_ACTIVE = 29.97  # threads per executed warp instruction, same capture
