@@ -294,15 +294,30 @@ __device__ __forceinline__ void rotate_to_axis(float ox, float oy, float oz, flo
   const float den = up ? 1.f + oz : s2 + 1e-30f;  // finite at o = -e_z, where q = 0
   const float num = up ? 1.f : 1.f - oz;
   const float t = q * num * rcp(den);
-  float x = fmaf(nx, oz, fmaf(ox, nz, -oy * t));
-  const float y = fmaf(ny, oz, fmaf(oy, nz, ox * t));
   const float z = fmaf(nz, oz, -fmaf(ox, nx, oy * ny));
-  // o = -e_z exactly: the formula gives (-n_x, -n_y, -n_z), the reference (n_x, -n_y, -n_z)
-  if (kExactNegZ && !up && s2 == 0.f) x = nx;
-  const float f = fmaf(-0.5f, fmaf(x, x, fmaf(y, y, z * z)), 1.5f);
-  rx = x * f;
-  ry = y * f;
-  rz = z * f;
+  if constexpr (kExactNegZ) {
+    float x = fmaf(nx, oz, fmaf(ox, nz, -oy * t));
+    const float y = fmaf(ny, oz, fmaf(oy, nz, ox * t));
+    // o = -e_z exactly: the formula gives (-n_x, -n_y, -n_z), the reference (n_x, -n_y, -n_z)
+    if (!up && s2 == 0.f) x = nx;
+    const float f = fmaf(-0.5f, fmaf(x, x, fmaf(y, y, z * z)), 1.5f);
+    rx = x * f;
+    ry = y * f;
+    rz = z * f;
+  } else {
+    // the compat-mode step's turn: the (x, y) rows and the renormalisation on
+    // sm_100's packed FP32 instructions (round to nearest, so the same bits
+    // as the scalar form above); the emission keeps the scalar form, which
+    // the batched kernel's 64-register loop runs faster
+    const float2 xy = __ffma2_rn(make_float2(nx, ny), make_float2(oz, oz),
+                                 __ffma2_rn(make_float2(ox, oy), make_float2(nz, nz),
+                                            __fmul2_rn(make_float2(-oy, ox), make_float2(t, t))));
+    const float f = fmaf(-0.5f, fmaf(xy.x, xy.x, fmaf(xy.y, xy.y, z * z)), 1.5f);
+    const float2 rxy = __fmul2_rn(xy, make_float2(f, f));
+    rx = rxy.x;
+    ry = rxy.y;
+    rz = z * f;
+  }
 }
 
 // Per-launch constants.
